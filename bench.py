@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Benchmark of the projection engine on its headline workload.
+
+Workload (one step): fan-beam forward projection followed by the matched
+backprojection of a 2048 x 2048 float32 ellipse phantom; 1440 views over
+[0, 2 pi), 2048 detectors of unit pitch at the isocentre, source 8192 px from
+the isocentre.  Unit: Gray-px/s = 1e9 ray-pixel updates per second, an update
+being one nonzero entry of the projection operator visited (counted exactly on
+the device; forward and backward counts summed).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs N independent replicas (the engine is single-GPU; slices shard
+with no collective), launched by torchrun; value = all ranks' updates / the
+slowest rank's time.  --impl reference times the reference's own CPU projector
+(prj/cpuPrj.c compiled unchanged into oracle/_ref) on the host cores.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+adjoint Gray-px/s & BHC grad-iter/s vs plain path, 1 B200, rel err≤1e-5"
+WORKLOAD = dict(workload="fan-beam fwd+backprojection 2048^2, 1440 views/[0,2pi), 2048 bins, "
+                         "d=8192 px, float32 ellipse phantom",
+                n=2048, prjWidth=2048, np=1440, prjFull=1440, dSize=1.0, effectiveRate=1.0, d=8192.0)
+# quarter-scale sample of the same geometry for the CPU legs (same views and
+# detector pitch, n = prjWidth = 1024, same magnification)
+CPU_SAMPLE = dict(n=1024, prjWidth=1024, np=1440, prjFull=1440, dSize=1.0, effectiveRate=1.0,
+                  d=4096.0)
+L2_FLUSH_BYTES = 512 << 20   # > 126 MB L2
+
+
+def geometry_tuple(w):
+    return (w["n"], w["prjWidth"], w["np"], w["prjFull"], w["dSize"], w["effectiveRate"], w["d"])
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples for one GPU while running."""
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8 or (self.uuid and self.uuid not in parts[0]):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def init_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_run(steps, warmup, threads=None):
+    """The reference's own prj/cpuPrj.c (oracle/_ref) -- or, where it was not
+    compiled, the oracle's FP32 port -- on the quarter-scale sample: each step
+    is one forward and one backward pass.  Returns (updates/s, seconds, info)."""
+    import types
+
+    import numpy as np
+
+    import oracle
+    from oracle import ref
+    from imgrecsrc_b200 import phantom
+    g = types.SimpleNamespace(**CPU_SAMPLE)
+    x = phantom.ellipse_phantom(g.n, seed=1)
+    nnz = oracle.forward_nnz(g) + oracle.backward_nnz(g)
+    ncores = os.cpu_count() or 1
+    if ref.available("libref_prj32"):
+        kind, cores = "reference", min(64, ncores)   # cpuPrj.c runs 64 pthreads
+
+        def step():
+            s = ref.forward(g, x, prec=32)
+            ref.backward(g, s, prec=32)
+    else:
+        kind, cores = "port", ncores
+
+        def step():
+            s = oracle.forward(g, x, prec=32, threads=ncores)
+            oracle.backward(g, s, prec=32, threads=ncores)
+    for _ in range(warmup):
+        step()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    sample = ("fan %d^2, %d views/[0,2pi), %d bins, d=%g px (quarter-scale of the workload): "
+              "one forward + one backward pass per step, %d timed; %d nonzero updates per step; "
+              "host has %d cores" % (g.n, g.np, g.prjWidth, g.d, steps, nnz, ncores))
+    return nnz / t / 1e9, t, dict(kind=kind, cores=cores, sample=sample)
+
+
+def reference_arm(args):
+    world, rank, _ = init_dist()
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 5))
+    warmup = max(0, min(args.warmup, 1))
+    v, t, info = cpu_reference_run(steps, warmup)
+    line = {"metric": METRIC, "value": v, "unit": "Gray-px/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference", "config": dict(WORKLOAD, sample=info["sample"]),
+            "cpu_baseline": dict(value=v, unit="Gray-px/s", **info),
+            "e2e": {"value": v, "unit": "Gray-px/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def our_arm(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = init_dist()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    import imgrecsrc_b200 as ct
+    from imgrecsrc_b200 import phantom
+
+    g = ct.Geometry(*geometry_tuple(WORKLOAD))
+    pr = ct.Projector(g, device=local)
+    nnz_f, nnz_b = pr.count_updates()
+    x = torch.from_numpy(phantom.ellipse_phantom(g.n, seed=1)).cuda()
+    sino = torch.empty(g.np, g.prjWidth, device="cuda")
+    back = torch.empty(g.n, g.n, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        pr.forward(x, out=sino)
+        pr.backward(sino, out=back)
+
+    for _ in range(max(3, args.warmup)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()                     # L2 flushed between timed steps (outside the events)
+        ev[i][0].record(stream)
+        pr.forward(x, out=sino)
+        ev[i][1].record(stream)
+        pr.backward(sino, out=back)
+        ev[i][2].record(stream)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    t_fwd = [ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)]
+    t_bwd = [ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)]
+    t_step = sum(a + b for a, b in zip(t_fwd, t_bwd)) / args.steps   # ms
+    t_max = t_step
+    if pg:
+        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = world * (nnz_f + nnz_b) / (t_max * 1e-3) / 1e9
+
+    # roofline of the dominant kernel: 4 B per update + the compulsory image and
+    # sinogram streams; duration from the CUDA events around its launch
+    fwd_ms, bwd_ms = statistics.mean(t_fwd), statistics.mean(t_bwd)
+    compulsory = 4 * (g.n * g.n + g.np * g.prjWidth)
+    if bwd_ms >= fwd_ms:
+        kname, kms, kbytes = "k_backward<fan>", bwd_ms, 4 * nnz_b + compulsory
+    else:
+        kname, kms, kbytes = "k_transpose + k_forward<fan>", fwd_ms, 4 * nnz_f + compulsory + 8 * g.n * g.n
+    peak, peak_kind = peaks()
+    achieved = kbytes / (kms * 1e-3) / 1e9
+    traffic = PROFILED_TRAFFIC.get("k_backward" if bwd_ms >= fwd_ms else "k_forward")
+
+    # end to end through the reference-facing C ABI: setup() once, then per
+    # step gpuPrj(FWD) and gpuPrj(BWD) on pinned host buffers (every call
+    # copies its input to the device and its result back, as the reference does)
+    os.environ["CTPRJ_DEVICE"] = str(local)
+    L = ct.lib()
+    L.setup(*geometry_tuple(WORKLOAD))
+    h_img = torch.from_numpy(phantom.ellipse_phantom(g.n, seed=1)).pin_memory()
+    h_sino = torch.empty(g.np, g.prjWidth).pin_memory()
+    h_back = torch.empty(g.n, g.n).pin_memory()
+    for _ in range(2):
+        ct.check(L.gpuPrj(ctypes.c_void_p(h_img.data_ptr()), ctypes.c_void_p(h_sino.data_ptr()), bytes([ct.FWD_BIT])))
+        ct.check(L.gpuPrj(ctypes.c_void_p(h_back.data_ptr()), ctypes.c_void_p(h_sino.data_ptr()), bytes([ct.BWD_BIT])))
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ct.check(L.gpuPrj(ctypes.c_void_p(h_img.data_ptr()), ctypes.c_void_p(h_sino.data_ptr()), bytes([ct.FWD_BIT])))
+        ct.check(L.gpuPrj(ctypes.c_void_p(h_back.data_ptr()), ctypes.c_void_p(h_sino.data_ptr()), bytes([ct.BWD_BIT])))
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_t = statistics.mean(e2e_times)
+    if pg:
+        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e_val = world * (nnz_f + nnz_b) / e2e_t / 1e9
+    img_b, sino_b = 4 * g.n * g.n, 4 * g.np * g.prjWidth
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gray-px/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t_max,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded ellipse phantom)",
+        "config": dict(WORKLOAD, l2="flushed between timed steps (512 MiB write)",
+                       parallelism="replicas" if world > 1 else "single GPU",
+                       updates_per_step={"forward": nnz_f, "backward": nnz_b},
+                       fwd_ms=fwd_ms, bwd_ms=bwd_ms),
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "bytes_per_launch": kbytes, "bytes_rule": "4 B per nonzero update + image + sinogram"},
+        "e2e": {"value": e2e_val, "unit": "Gray-px/s", "h2d_bytes_per_step": img_b + sino_b,
+                "d2h_bytes_per_step": sino_b + img_b, "api": "setup()/gpuPrj() C ABI, pinned host buffers",
+                "ms_per_step": e2e_t * 1e3},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, t, info = cpu_reference_run(1, 0)
+        line["cpu_baseline"] = dict(value=v, unit="Gray-px/s", **info)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from the ncu
+# captures summarised in profiles/ (None until captured)
+PROFILED_TRAFFIC = {}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,83 @@
+"""ctypes binding of libctprj.so, the engine's C ABI (include/ctprj.h).
+
+The library is built in-tree by imgrecsrc_b200/build.py.  There is no CPU
+fallback: importing a compute entry point without the library raises.
+"""
+import ctypes
+import os
+
+from .build import LIB
+
+CTPRJ_OK, CTPRJ_EINVAL, CTPRJ_ENOTSETUP, CTPRJ_ENOMEM, CTPRJ_ECUDA, CTPRJ_ERANGE, CTPRJ_ETIMEOUT = range(7)
+FWD_BIT, BWD_BIT, FBP_BIT = 1 << 1, 1 << 2, 1 << 3
+
+
+class CtprjError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("ctprj status %d: %s" % (status, message))
+        self.status = status
+
+
+class Geometry(ctypes.Structure):
+    """struct ctprj_geometry -- the reference's projector configuration
+    (prj/prj.h:42-57): n, prjWidth, np, prjFull, dSize, effectiveRate, d."""
+    _fields_ = [("n", ctypes.c_int), ("prjWidth", ctypes.c_int), ("np", ctypes.c_int),
+                ("prjFull", ctypes.c_int), ("dSize", ctypes.c_float),
+                ("effectiveRate", ctypes.c_float), ("d", ctypes.c_float)]
+
+    def __init__(self, n, prjWidth, np, prjFull, dSize=1.0, effectiveRate=1.0, d=0.0):
+        super().__init__(int(n), int(prjWidth), int(np), int(prjFull), float(dSize),
+                         float(effectiveRate), float(d))
+
+    @property
+    def fan(self):
+        return self.d > 0
+
+    def as_tuple(self):
+        return (self.n, self.prjWidth, self.np, self.prjFull, self.dSize, self.effectiveRate, self.d)
+
+    def __repr__(self):
+        return ("Geometry(n=%d, prjWidth=%d, np=%d, prjFull=%d, dSize=%g, effectiveRate=%g, d=%g)"
+                % self.as_tuple())
+
+
+_lib = None
+VP = ctypes.c_void_p
+
+
+def lib():
+    """The loaded libctprj.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        raise RuntimeError("libctprj.so is missing: build it with `python -m imgrecsrc_b200.build`")
+    L = ctypes.CDLL(LIB)
+    GP = ctypes.POINTER(Geometry)
+    sig = {
+        "setup": ([ctypes.c_int] * 4 + [ctypes.c_float] * 3, None),
+        "showSetup": ([], None),
+        "gpuPrj": ([VP, VP, ctypes.c_char], ctypes.c_int),
+        "ctprj_plan_create": ([GP, ctypes.c_int, ctypes.POINTER(VP)], ctypes.c_int),
+        "ctprj_plan_destroy": ([VP], None),
+        "ctprj_forward": ([VP, VP, VP, VP], ctypes.c_int),
+        "ctprj_backward": ([VP, VP, VP, VP], ctypes.c_int),
+        "ctprj_fbp": ([VP, VP, VP, VP], ctypes.c_int),
+        "ctprj_count_updates": ([VP, ctypes.POINTER(ctypes.c_longlong),
+                                 ctypes.POINTER(ctypes.c_longlong), VP], ctypes.c_int),
+        "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
+        "ctprj_last_error": ([], ctypes.c_char_p),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != CTPRJ_OK:
+        L = lib()
+        raise CtprjError(status, (L.ctprj_last_error() or L.ctprj_error_string(status)).decode())
+    return status

@@ -1,0 +1,434 @@
+// api.cu -- C ABI of the projection engine: plans, the reference-compatible
+// setup()/showSetup()/gpuPrj() entry points, and error reporting.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "ctprj_internal.h"
+#include "footprint.cuh"
+
+namespace ctprj {
+
+static thread_local char t_err[512] = "";
+
+int set_error(int status, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_err, sizeof t_err, fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+int cuda_error(cudaError_t e, const char *what)
+{
+    if (e == cudaSuccess) return CTPRJ_OK;
+    if (e == cudaErrorMemoryAllocation)
+        return set_error(CTPRJ_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+    return set_error(CTPRJ_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// View angle of view i exactly as the reference forms it (prj/cpuPrj.c:342):
+// ((float)(2 i) * pi_f) / (float)prjFull in float arithmetic.
+static double view_angle(int i, int P)
+{
+    volatile float th = (float)(2 * i) * kRefPiF;
+    th = th / (float)P;
+    return (double)th;
+}
+
+// View of symmetric image j for base view b: (q_j P/4 + s_j b) mod P, with
+// (q, s) = (0,+)(1,+)(2,+)(3,+)(2,-)(3,-)(4,-)(1,-) (prj/cpuPrj.c:403-460,
+// :117-157).
+static int view_of(int j, int b, int P)
+{
+    static const int q[8] = {0, 1, 2, 3, 2, 3, 4, 1};
+    static const int sg[8] = {1, 1, 1, 1, -1, -1, -1, -1};
+    int v = (q[j] * (P / 4) + sg[j] * b) % P;
+    return v < 0 ? v + P : v;
+}
+
+static int validate(const ctprj_geometry *g)
+{
+    if (!g) return set_error(CTPRJ_EINVAL, "geometry is NULL");
+    if (g->n < 1 || g->prjWidth < 1 || g->np < 1)
+        return set_error(CTPRJ_EINVAL, "n, prjWidth and np must be positive (n=%d prjWidth=%d np=%d)",
+                         g->n, g->prjWidth, g->np);
+    if (g->prjFull < 4 || g->prjFull % 4 != 0)
+        return set_error(CTPRJ_EINVAL, "prjFull must be a positive multiple of 4 (prjFull=%d)",
+                         g->prjFull);
+    if (g->np > g->prjFull)
+        return set_error(CTPRJ_EINVAL, "np (%d) exceeds prjFull (%d)", g->np, g->prjFull);
+    if (!(g->dSize > 0.0f) || !std::isfinite(g->dSize))
+        return set_error(CTPRJ_EINVAL, "dSize must be positive and finite");
+    if (!(g->effectiveRate > 0.0f) || !std::isfinite(g->effectiveRate))
+        return set_error(CTPRJ_EINVAL, "effectiveRate must be positive and finite");
+    if (!std::isfinite(g->d)) return set_error(CTPRJ_EINVAL, "d must be finite");
+    if ((long long)g->n * g->n >= (1LL << 31) || (long long)g->np * g->prjWidth >= (1LL << 31) ||
+        (long long)g->prjFull * g->prjWidth >= (1LL << 31))
+        return set_error(CTPRJ_ERANGE, "image or sinogram exceeds 2^31 elements");
+    if (g->n > 65536 || g->prjWidth > 65536)
+        return set_error(CTPRJ_ERANGE, "n and prjWidth are limited to 65536");
+    return CTPRJ_OK;
+}
+
+static Geo make_geo(const ctprj_geometry &gm)
+{
+    Geo g;
+    g.n = gm.n;
+    g.W = gm.prjWidth;
+    g.np = gm.np;
+    g.P = gm.prjFull;
+    g.pC = gm.prjWidth / 2;
+    g.half = (gm.n - 1) / 2;
+    g.h2 = gm.n / 2;
+    g.fan = gm.d > 0.0f;
+    g.dSize = gm.dSize;
+    g.beamWidth = (double)gm.dSize * (double)gm.effectiveRate;
+    g.d = gm.d;
+    g.beamWidthF = (float)g.beamWidth;
+    g.dF = gm.d;
+    g.invEr = 1.0f / gm.effectiveRate;
+    g.effRate = gm.effectiveRate;
+    return g;
+}
+
+template <class T>
+static int upload(T **dst, const std::vector<T> &src)
+{
+    int st = cuda_error(cudaMalloc((void **)dst, sizeof(T) * (src.empty() ? 1 : src.size())),
+                        "table allocation");
+    if (st) return st;
+    if (!src.empty())
+        st = cuda_error(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice),
+                        "table upload");
+    return st;
+}
+
+static void free_plan(ctprj_plan *p)
+{
+    if (!p) return;
+    cudaFree(p->d_fview);
+    cudaFree(p->d_bview);
+    cudaFree(p->d_det);
+    cudaFree(p->d_imgT);
+    cudaFree(p->d_count);
+    cudaFree(p->d_ramp);
+    cudaFree(p->d_fsino);
+    delete p;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    bool changed = false;
+    int status = CTPRJ_OK;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (dev >= 0 && dev != prev) {
+            status = cuda_error(cudaSetDevice(dev), "cudaSetDevice");
+            changed = status == CTPRJ_OK;
+        }
+    }
+    ~DeviceGuard()
+    {
+        if (changed && prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+static int build_plan(const ctprj_geometry *geom, int device, ctprj_plan **out)
+{
+    int st = validate(geom);
+    if (st) return st;
+    ctprj_plan *p = new (std::nothrow) ctprj_plan();
+    if (!p) return set_error(CTPRJ_ENOMEM, "host allocation failed");
+    memset(p, 0, sizeof *p);
+    p->geom = *geom;
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) device = 0;
+    p->device = device;
+    p->g = make_geo(*geom);
+    const Geo &g = p->g;
+    const int W = g.W, P = g.P, np = g.np;
+
+    // forward ray set (prj/cpuPrj.c:326-332, :469-475, :632-644)
+    p->nb = np < P / 8 + 1 ? np : P / 8 + 1;
+    p->k0 = (W % 2 == 0) ? 1 : 0;
+    p->nk = g.fan ? (W % 2 == 0 ? W - 1 : W) : (W % 2 == 0 ? W / 2 : (W + 1) / 2);
+    p->nv = g.fan ? P : P / 2;
+
+    std::vector<FwdView> fv(p->nb);
+    for (int b = 0; b < p->nb; ++b) {
+        const double th = view_angle(b, P);
+        fv[b].c = cos(th);
+        fv[b].s = sin(th);
+        const bool mirror = b > 0 && (float)b < (float)P * 0.125f;
+        for (int j = 0; j < 8; ++j) {
+            const int v = view_of(j, b, P);
+            fv[b].out[j] = ((j < 4 || mirror) && v < np) ? v : -1;
+        }
+    }
+    std::vector<BwdView> bv(p->nv);
+    for (int i = 0; i < p->nv; ++i) {
+        BwdView &e = bv[i];
+        const double th = view_angle(i, P);
+        e.c = cos(th);
+        e.s = sin(th);
+        e.cf = (float)e.c;
+        e.sf = (float)e.s;
+        const Footprint f = make_footprint(e.cf, e.sf);
+        e.h = f.h; e.b1 = f.b1; e.b2 = f.b2; e.w = f.w; e.iw2 = f.iw2; e.pad = 0;
+        e.cnt4 = e.cnt8 = 0;
+        for (int j = 0; j < 8; ++j) {
+            const int v = view_of(j, i, P);
+            e.row[j] = v < np ? v * W : -1;
+            int v2 = (v + P / 2) % P;
+            e.row2[j] = (!g.fan && v2 < np) ? v2 * W : -1;
+            const int reads = (e.row[j] >= 0) + (e.row2[j] >= 0);
+            e.cnt8 += reads;
+            if (j < 4) e.cnt4 += reads;
+        }
+    }
+    std::vector<DetEntry> de(W);
+    for (int k = 0; k < W; ++k) {
+        DetEntry &e = de[k];
+        e.t = (double)(k - g.pC) * g.dSize;
+        if (g.fan) {
+            const double bq = sqrt(g.d * g.d + e.t * e.t);
+            e.cB = g.d / bq;
+            e.sB = e.t / bq;
+            e.invbq = (float)(1.0 / bq);
+        } else {
+            e.cB = 1.0;
+            e.sB = 0.0;
+            e.invbq = 0.0f;
+        }
+        e.cBf = (float)e.cB;
+        e.sBf = (float)e.sB;
+        e.pad = 0;
+    }
+
+    DeviceGuard dg(device);
+    if ((st = dg.status)) { delete p; return st; }
+    if ((st = upload(&p->d_fview, fv)) || (st = upload(&p->d_bview, bv)) ||
+        (st = upload(&p->d_det, de)) ||
+        (st = cuda_error(cudaMalloc((void **)&p->d_imgT, sizeof(float) * (size_t)g.n * g.n),
+                         "scratch allocation")) ||
+        (st = cuda_error(cudaMalloc((void **)&p->d_count, sizeof(unsigned long long)),
+                         "counter allocation"))) {
+        free_plan(p);
+        return st;
+    }
+    *out = p;
+    return CTPRJ_OK;
+}
+
+}  // namespace ctprj
+
+using namespace ctprj;
+
+// ------------------------------------------------------------------ plan API
+
+extern "C" int ctprj_plan_create(const ctprj_geometry *geom, int device, ctprj_plan **plan)
+{
+    if (!plan) return set_error(CTPRJ_EINVAL, "plan output pointer is NULL");
+    *plan = nullptr;
+    return build_plan(geom, device, plan);
+}
+
+extern "C" void ctprj_plan_destroy(ctprj_plan *plan)
+{
+    if (!plan) return;
+    DeviceGuard dg(plan->device);
+    free_plan(plan);
+}
+
+extern "C" int ctprj_forward(ctprj_plan *plan, const float *d_img, float *d_sino, void *stream)
+{
+    if (!plan || !d_img || !d_sino) return set_error(CTPRJ_EINVAL, "NULL plan or buffer");
+    DeviceGuard dg(plan->device);
+    if (dg.status) return dg.status;
+    cudaStream_t s = (cudaStream_t)stream;
+    int st = launch_transpose(d_img, plan->d_imgT, plan->g.n, s);
+    if (st) return st;
+    return launch_forward(plan, d_img, plan->d_imgT, d_sino, nullptr, s);
+}
+
+extern "C" int ctprj_backward(ctprj_plan *plan, const float *d_sino, float *d_img, void *stream)
+{
+    if (!plan || !d_img || !d_sino) return set_error(CTPRJ_EINVAL, "NULL plan or buffer");
+    DeviceGuard dg(plan->device);
+    if (dg.status) return dg.status;
+    return launch_backward(plan, d_sino, d_img, 0, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int ctprj_count_updates(ctprj_plan *plan, long long *fwd, long long *bwd, void *stream)
+{
+    if (!plan) return set_error(CTPRJ_EINVAL, "NULL plan");
+    DeviceGuard dg(plan->device);
+    if (dg.status) return dg.status;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned long long h[2] = {0, 0};
+    int st;
+    for (int pass = 0; pass < 2; ++pass) {
+        if ((st = cuda_error(cudaMemsetAsync(plan->d_count, 0, sizeof(unsigned long long), s),
+                             "counter reset")))
+            return st;
+        st = pass == 0 ? launch_forward(plan, nullptr, nullptr, nullptr, plan->d_count, s)
+                       : launch_backward(plan, nullptr, nullptr, 0, plan->d_count, s);
+        if (st) return st;
+        if ((st = cuda_error(cudaMemcpyAsync(&h[pass], plan->d_count, sizeof(unsigned long long),
+                                             cudaMemcpyDeviceToHost, s),
+                             "counter readback")) ||
+            (st = cuda_error(cudaStreamSynchronize(s), "counter sync")))
+            return st;
+    }
+    if (fwd) *fwd = (long long)h[0];
+    if (bwd) *bwd = (long long)h[1];
+    return CTPRJ_OK;
+}
+
+extern "C" const char *ctprj_error_string(int status)
+{
+    switch (status) {
+    case CTPRJ_OK: return "success";
+    case CTPRJ_EINVAL: return "invalid argument";
+    case CTPRJ_ENOTSETUP: return "setup() has not completed successfully";
+    case CTPRJ_ENOMEM: return "out of memory";
+    case CTPRJ_ECUDA: return "CUDA error";
+    case CTPRJ_ERANGE: return "size out of range";
+    case CTPRJ_ETIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char *ctprj_last_error(void) { return t_err; }
+
+// ----------------------------------------------- reference-compatible entry points
+
+static std::mutex g_mu;
+static struct prjConf g_conf;
+extern "C" {
+struct prjConf *pConf = &g_conf;
+}
+static ctprj_plan *g_plan = nullptr;
+static float *g_dimg = nullptr, *g_dsino = nullptr;
+static int g_status = CTPRJ_ENOTSETUP;
+static char g_msg[512] = "setup() has not been called";
+
+// prj/gpuPrj.cu:833-847: on a multi-GPU node the reference runs on the device
+// with the most multiprocessors.  The environment variable CTPRJ_DEVICE, when
+// set to a valid ordinal, selects the device instead (one process per GPU).
+static int pick_device()
+{
+    int n = 0, best = 0, best_sm = -1;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) return -1;
+    if (const char *env = getenv("CTPRJ_DEVICE")) {
+        char *end = nullptr;
+        long d = strtol(env, &end, 10);
+        if (end != env && d >= 0 && d < n) return (int)d;
+    }
+    for (int d = 0; d < n; ++d) {
+        int sm = 0;
+        if (cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, d) == cudaSuccess &&
+            sm > best_sm) {
+            best_sm = sm;
+            best = d;
+        }
+    }
+    return best;
+}
+
+static void release_global()
+{
+    if (g_plan) {
+        DeviceGuard dg(g_plan->device);
+        cudaFree(g_dimg);
+        cudaFree(g_dsino);
+        free_plan(g_plan);
+    }
+    g_plan = nullptr;
+    g_dimg = g_dsino = nullptr;
+}
+
+extern "C" void setup(int n, int prjWidth, int np, int prjFull, float dSize, float effectiveRate,
+                      float d)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_conf.n = n;
+    g_conf.prjWidth = prjWidth;
+    g_conf.np = np;
+    g_conf.prjFull = prjFull;
+    g_conf.dSize = dSize;
+    g_conf.effectiveRate = effectiveRate;
+    g_conf.d = d;
+    g_conf.cmd = 0;
+    g_conf.imgSize = (unsigned)n * (unsigned)n;
+    g_conf.sinoSize = (unsigned)prjWidth * (unsigned)np;
+    release_global();
+    ctprj_geometry gm = {n, prjWidth, np, prjFull, dSize, effectiveRate, d};
+    int dev = pick_device();
+    if (dev < 0) {
+        g_status = set_error(CTPRJ_ECUDA, "no CUDA device");
+    } else {
+        g_status = build_plan(&gm, dev, &g_plan);
+        if (g_status == CTPRJ_OK) {
+            DeviceGuard dg(dev);
+            g_status = cuda_error(cudaMalloc((void **)&g_dimg, sizeof(float) * (size_t)n * n),
+                                  "image buffer");
+            if (!g_status)
+                g_status = cuda_error(
+                    cudaMalloc((void **)&g_dsino, sizeof(float) * (size_t)np * prjWidth),
+                    "sinogram buffer");
+            if (g_status) release_global();
+        }
+    }
+    snprintf(g_msg, sizeof g_msg, "%s", g_status ? ctprj_last_error() : "");
+}
+
+extern "C" void showSetup(void)
+{
+    printf("config.n=%d\n", g_conf.n);
+    printf("config.prjWidth=%d\n", g_conf.prjWidth);
+    printf("config.np=%d\n", g_conf.np);
+    printf("config.prjFull=%d\n", g_conf.prjFull);
+    printf("config.dSize=%g\n", g_conf.dSize);
+    printf("config.effectiveRate=%g\n", g_conf.effectiveRate);
+    printf("config.d=%g\n", g_conf.d);
+}
+
+int ctprj_fbp_device(ctprj_plan *plan, const float *d_sino, float *d_img, cudaStream_t s);
+
+extern "C" int gpuPrj(float *img, float *sino, char cmd)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_status != CTPRJ_OK) return set_error(g_status, "%s", g_msg);
+    if (!img || !sino) return set_error(CTPRJ_EINVAL, "NULL image or sinogram pointer");
+    DeviceGuard dg(g_plan->device);
+    if (dg.status) return dg.status;
+    const size_t ib = sizeof(float) * g_conf.imgSize, sb = sizeof(float) * g_conf.sinoSize;
+    cudaStream_t s = 0;
+    int st;
+    if (cmd & FWD_BIT) {
+        if ((st = cuda_error(cudaMemcpyAsync(g_dimg, img, ib, cudaMemcpyHostToDevice, s), "image upload")) ||
+            (st = ctprj_forward(g_plan, g_dimg, g_dsino, s)) ||
+            (st = cuda_error(cudaMemcpyAsync(sino, g_dsino, sb, cudaMemcpyDeviceToHost, s), "sinogram download")))
+            return st;
+    } else if (cmd & BWD_BIT) {
+        if ((st = cuda_error(cudaMemcpyAsync(g_dsino, sino, sb, cudaMemcpyHostToDevice, s), "sinogram upload")) ||
+            (st = ctprj_backward(g_plan, g_dsino, g_dimg, s)) ||
+            (st = cuda_error(cudaMemcpyAsync(img, g_dimg, ib, cudaMemcpyDeviceToHost, s), "image download")))
+            return st;
+    } else if (cmd & FBP_BIT) {
+        if ((st = cuda_error(cudaMemcpyAsync(g_dsino, sino, sb, cudaMemcpyHostToDevice, s), "sinogram upload")) ||
+            (st = ctprj_fbp_device(g_plan, g_dsino, g_dimg, s)) ||
+            (st = cuda_error(cudaMemcpyAsync(img, g_dimg, ib, cudaMemcpyDeviceToHost, s), "image download")))
+            return st;
+    } else {
+        return CTPRJ_OK;   // the reference does nothing for other commands
+    }
+    return cuda_error(cudaStreamSynchronize(s), "gpuPrj synchronize");
+}

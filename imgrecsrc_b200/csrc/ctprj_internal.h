@@ -1,0 +1,104 @@
+// ctprj_internal.h -- plan layout, geometry tables and kernel parameter
+// blocks shared by the host code and the sm_100a kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/ctprj.h"
+
+namespace ctprj {
+
+// The reference's pi is the float literal 3.14159265359f (prj/prj.h:9) and view
+// angles are formed in float arithmetic, fl(fl(2i * pi_f) / prjFull), in both of
+// its precisions (prj/cpuPrj.c:342).  View tables are built on the host from
+// exactly that value, with cos/sin evaluated in double.
+constexpr float kRefPiF = 3.14159265359f;
+
+// Forward base view (0 <= b <= prjFull/8): its direction and, for each of the
+// eight symmetric images j (order of prj/cpuPrj.c:383-397), the sinogram row it
+// is written to, or -1.  Images 4..7 also mirror the detector.
+struct FwdView {
+    double c, s;
+    int out[8];
+};
+
+// Backward base view i (all views for fan beam, the first half for parallel
+// beam, prj/cpuPrj.c:76, :213): direction, the sinogram row offsets
+// (view * prjWidth, or -1) read for each image j, and for parallel beam the
+// rows of the opposite views (view + prjFull/2) read with the detector
+// mirrored.  shape = footprint of the parallel ray (unused for fan beam).
+struct BwdView {
+    double c, s;
+    float cf, sf;
+    float h, b1, b2, w, iw2, pad;
+    int row[8];
+    int row2[8];
+    int cnt4, cnt8;   // valid reads per weight for 4 / 8 distinct images
+};
+
+// Detector k: t = (k - prjWidth/2) * dSize and, for fan beam, the direction
+// of its ray relative to the central ray (cos B = d/bq, sin B = t/bq).
+struct DetEntry {
+    double t, cB, sB;
+    float cBf, sBf, invbq, pad;
+};
+
+struct Geo {
+    int n, W, np, P;
+    int pC, half, h2;        // prjWidth/2, (n-1)/2, n/2
+    int fan;
+    double dSize, beamWidth, d;
+    float beamWidthF, dF, invEr;
+    float effRate;
+};
+
+struct FwdParams {
+    Geo g;
+    int nb, k0, nk;           // base views, first ray, rays per base view
+    int zero_col0;            // even prjWidth: detector 0 written as zero
+    const FwdView *view;
+    const DetEntry *det;
+};
+
+struct BwdParams {
+    Geo g;
+    int nv;                   // base views looped over
+    int tiles_side;
+    int zero_axes;            // even n: row 0 and column 0 written as zero
+    float fbp_scale;          // FBP: PI_f/np/dSize/dSize, else 1
+    const BwdView *view;
+    const DetEntry *det;
+};
+
+}  // namespace ctprj
+
+struct ctprj_plan {
+    ctprj_geometry geom;
+    int device;
+    ctprj::Geo g;
+    int nb, k0, nk;           // forward ray set (prj/cpuPrj.c:326-332, :469-475)
+    int nv;                   // backward view count
+    ctprj::FwdView *d_fview;
+    ctprj::BwdView *d_bview;
+    ctprj::DetEntry *d_det;
+    float *d_imgT;            // scratch: transposed image (n*n)
+    unsigned long long *d_count;
+    // FBP: ramp-filter taps (2*prjWidth) and filtered-sinogram scratch
+    float *d_ramp;
+    float *d_fsino;
+};
+
+namespace ctprj {
+
+int set_error(int status, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+
+// launchers (projector.cu)
+int launch_transpose(const float *src, float *dst, int n, cudaStream_t s);
+int launch_forward(const ctprj_plan *p, const float *img, const float *imgT, float *sino,
+                   unsigned long long *counter, cudaStream_t s);
+int launch_backward(const ctprj_plan *p, const float *sino, float *img, int fbp,
+                    unsigned long long *counter, cudaStream_t s);
+
+}  // namespace ctprj

@@ -1,0 +1,62 @@
+"""Host mirror of the reference's MATLAB operator interface.
+
+``gpuPrj(x, conf, cmd)`` follows the MEX gateway prj/mPrj.c:37-173 (built by
+the reference as gpuPrj.mex): ``cmd`` is 'config' (conf carries the fields n,
+prjWidth, np, prjFull, dSize, effectiveRate, d), 'forward', 'backward', 'FBP',
+or anything else to print the configuration.  Arrays are taken and returned
+with MATLAB's meaning: an image argument is the n x n matrix (rows are y),
+passed as a 2-D array or as its column-major vector; a sinogram is the
+prjWidth*np vector, view after view.  Results are float64 vectors, as the MEX
+function returns, in MATLAB's column-major order.  The work runs through the C
+ABI's setup()/gpuPrj() on the GPU; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import BWD_BIT, FBP_BIT, FWD_BIT, check, lib
+
+_conf = None
+
+
+def _field(conf, name):
+    return conf[name] if isinstance(conf, dict) else getattr(conf, name)
+
+
+def _image_in(x, n):
+    a = np.asarray(x)
+    if a.ndim == 2:
+        return np.ascontiguousarray(a, dtype=np.float32)
+    # a MATLAB column-major vector of the n x n matrix (prj/mPrj.c:82-84)
+    return np.ascontiguousarray(a.reshape(n, n, order="F"), dtype=np.float32)
+
+
+def gpuPrj(x, conf, cmd):
+    global _conf
+    L = lib()
+    if cmd == "config":
+        vals = [_field(conf, k) for k in ("n", "prjWidth", "np", "prjFull", "dSize",
+                                          "effectiveRate", "d")]
+        L.setup(int(vals[0]), int(vals[1]), int(vals[2]), int(vals[3]), float(vals[4]),
+                float(vals[5]), float(vals[6]))
+        _conf = dict(zip(("n", "prjWidth", "np", "prjFull", "dSize", "effectiveRate", "d"), vals))
+        return None
+    if _conf is None:
+        raise RuntimeError("gpuPrj: call with 'config' first")
+    n, W, npv = int(_conf["n"]), int(_conf["prjWidth"]), int(_conf["np"])
+    if cmd == "forward":
+        img = _image_in(x, n)
+        sino = np.zeros((npv, W), np.float32)
+        check(L.gpuPrj(img.ctypes.data, sino.ctypes.data, bytes([FWD_BIT])))
+        return sino.astype(np.float64).ravel()
+    if cmd in ("backward", "FBP"):
+        sino = np.ascontiguousarray(np.asarray(x, dtype=np.float32).ravel())
+        if sino.size != npv * W:
+            raise ValueError("expected a sinogram of %d values" % (npv * W))
+        img = np.zeros((n, n), np.float32)
+        bit = BWD_BIT if cmd == "backward" else FBP_BIT
+        check(L.gpuPrj(img.ctypes.data, sino.ctypes.data, bytes([bit])))
+        # column-major vector of the image matrix (prj/mPrj.c:134-136)
+        return img.astype(np.float64).ravel(order="F")
+    L.showSetup()
+    return None

@@ -166,3 +166,48 @@ def par_backward(y, mask_idx, conf, threads=0):
 
 
 from . import ref  # noqa: E402,F401
+
+
+_PI_F = np.float32(3.14159265359)
+
+
+def ramp_filter_rows(sino_rows):
+    """prj/utils.h:94-151 (rampFilter) applied to every row, in FP64: each row
+    of W samples is zero padded to N = 2W, multiplied in the DFT domain by the
+    real part of the DFT of the spatial ramp (0.25 at 0, -1/(pi^2 i^2) at odd
+    lags, formed in float as the reference does) times a Hann window
+    0.5 + 0.5 cos(2 pi i / N) (argument formed in float), and the first W
+    samples of the inverse DFT are kept."""
+    s = np.asarray(sino_rows, np.float64)
+    W = s.shape[-1]
+    N = 2 * W
+    ramp = np.zeros(N, np.float64)
+    ramp[0] = 0.25
+    for i in range(1, N):
+        if i % 2 == 0:
+            continue
+        m = i if i < N // 2 else N - i
+        r = np.float32(-1.0) / _PI_F
+        r = r / _PI_F
+        r = r / np.float32(m)
+        r = r / np.float32(m)
+        ramp[i] = float(r)
+    i = np.arange(N)
+    arg = ((np.float32(2.0) * _PI_F) * i.astype(np.float32)) / np.float32(N)
+    hann = 0.5 + 0.5 * np.cos(arg.astype(np.float64))
+    G = np.fft.fft(ramp).real * hann
+    pad = np.zeros(s.shape[:-1] + (N,), np.float64)
+    pad[..., :W] = s
+    return np.fft.ifft(np.fft.fft(pad, axis=-1) * G, axis=-1).real[..., :W]
+
+
+def fbp(g, sino, prec=64, threads=0):
+    """prj/cpuPrj.c:718-784 (cmd FBP_BIT): fan-beam cosine pre-weight
+    d / sqrt(d^2 + (j dSize)^2) at detector offset j, ramp filter per view,
+    then the FBP-weighted backprojection."""
+    s = np.asarray(sino, np.float64).reshape(g.np, g.prjWidth).copy()
+    if g.d > 0:
+        j = np.abs(np.arange(g.prjWidth) - g.prjWidth // 2).astype(np.float64)
+        d = float(g.d)
+        s *= d / np.sqrt(d * d + j * j * float(g.dSize) * float(g.dSize))
+    return backward(g, ramp_filter_rows(s), prec=prec, threads=threads, fbp_weighting=True)

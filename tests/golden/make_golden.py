@@ -1,7 +1,7 @@
 """Generates the golden fixtures in this directory from the reference itself.
 
-Runs the reference's own prj/cpuPrj.c (FP64-widened and as-shipped FP32) and
-prj/parPrj.c, compiled unchanged from the reference sources into oracle/_ref
+Runs the reference's own prj/cpuPrj.c (FP64-widened and as-shipped FP32:
+forward, backward and FBP) and prj/parPrj.c, compiled unchanged from the reference sources into oracle/_ref
 (``make -C oracle ref``), on small seeded inputs, and stores inputs and outputs
 in ``projector_golden.npz`` / ``parprj_golden.npz``.  The tests compare the
 oracle restatement and the GPU path against these files, so they need neither
@@ -63,6 +63,7 @@ def main():
         out["c%d_bwd64" % ci] = ref.backward(g, y, 64)
         out["c%d_fwd32" % ci] = ref.forward(g, x.astype(np.float32), 32)
         out["c%d_bwd32" % ci] = ref.backward(g, y.astype(np.float32), 32)
+        out["c%d_fbp64" % ci] = ref.fbp(g, y, 64)
     out["ncases"] = np.array(len(PROJECTOR_CASES))
     np.savez_compressed(os.path.join(os.path.dirname(__file__), "projector_golden.npz"), **out)
 

@@ -50,6 +50,15 @@ def test_fp64_restatement_matches_reference_fixtures(case):
 
 
 @pytest.mark.parametrize("case", range(10))
+def test_fbp_restatement_matches_reference_fixtures(case):
+    z = np.load(GOLD)
+    if case >= int(z["ncases"]):
+        pytest.skip("no such fixture")
+    g = geom(z["c%d_geom" % case])
+    assert rel(oracle.fbp(g, z["c%d_sino" % case]), z["c%d_fbp64" % case]) < 1e-12
+
+
+@pytest.mark.parametrize("case", range(10))
 def test_fp32_restatement_matches_reference_fixtures(case):
     z = np.load(GOLD)
     if case >= int(z["ncases"]):
