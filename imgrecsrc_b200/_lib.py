@@ -65,6 +65,12 @@ def lib():
         "ctprj_fbp": ([VP, VP, VP, VP], ctypes.c_int),
         "ctprj_count_updates": ([VP, ctypes.POINTER(ctypes.c_longlong),
                                  ctypes.POINTER(ctypes.c_longlong), VP], ctypes.c_int),
+        "ctprj_bhc_create": ([VP, ctypes.c_int, VP, ctypes.c_double, ctypes.POINTER(VP)], ctypes.c_int),
+        "ctprj_bhc_destroy": ([VP], None),
+        "ctprj_bhc_forward": ([VP, VP, VP, VP, VP, ctypes.c_int, VP], ctypes.c_int),
+        "ctprj_bhc_backward": ([VP, VP, VP, VP, VP, VP, VP], ctypes.c_int),
+        "ctprj_bhc_terms": ([VP, VP, VP, VP, VP, ctypes.c_int, VP], ctypes.c_int),
+        "ctprj_bhc_state": ([VP, ctypes.POINTER(VP), ctypes.POINTER(VP), ctypes.POINTER(VP)], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

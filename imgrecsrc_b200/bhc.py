@@ -1,0 +1,103 @@
+"""Polychromatic beam-hardening model over torch tensors (include/ctprj.h,
+ctprj_bhc_*), the GPU counterpart of bhc/Spline.m (b1Iout) with
+bhc/poissLAlpha.m and bhc/poissLI.m.
+
+Per ray i: s_i = Ts (A x)_i; BL_i = sum_j Ie_j b_j(s_i) over degree-1 B-spline
+basis functions on J + 2 mass-attenuation nodes; the Poisson negative
+log-likelihood f = sum_i BL_i - m_i - m_i log(BL_i / m_i) of the measured
+intensity m (counts / I0), and its gradients in x (through Ts A^T) and in Ie.
+Spline arithmetic and reductions are FP64 on the GPU.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import check, lib
+from .projector import _dev_ptr, _stream_handle
+
+
+def kappa_nodes(J, kmin=1e-2, kmax=1e2):
+    """J log-spaced values on [kmin, kmax] padded with one node on each side at
+    the grid's ratio (the node rule of bhc/beamhardenSpline.m:164-165)."""
+    kappa = np.logspace(np.log10(kmin), np.log10(kmax), J)
+    q = kappa[1] / kappa[0]
+    return np.concatenate([[kappa[0] / q], kappa, [kappa[-1] * q]])
+
+
+def _dptr(t, n, dtype):
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == dtype and t.is_contiguous()):
+        raise TypeError("expected a contiguous CUDA %s tensor" % dtype)
+    if t.numel() != n:
+        raise ValueError("expected %d elements, got %d" % (n, t.numel()))
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class BHCModel:
+    """Fused forward (projection + per-ray spline epilogue) and hand-written
+    adjoint on one Projector's geometry."""
+
+    def __init__(self, projector, nodes, Ts):
+        self.projector = projector
+        self.nodes = np.ascontiguousarray(nodes, np.float64)
+        self.J = self.nodes.size - 2
+        self.Ts = float(Ts)
+        self._m = ctypes.c_void_p()
+        check(lib().ctprj_bhc_create(projector._plan, self.J, self.nodes.ctypes.data,
+                                     self.Ts, ctypes.byref(self._m)))
+        g = projector.geometry
+        self.nrays = g.np * g.prjWidth
+
+    def close(self):
+        if self._m:
+            lib().ctprj_bhc_destroy(self._m)
+            self._m = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _args(self, x, Ie, imea):
+        import torch
+        pr = self.projector
+        return (_dev_ptr(x, pr.img_shape, pr.device) if x is not None else None,
+                _dptr(Ie, self.J, torch.float64) if Ie is not None else None,
+                _dptr(imea, self.nrays, torch.float32) if imea is not None else None)
+
+    def forward(self, x, Ie, imea, save=True, out=None, stream=None):
+        """f (a 1-element float64 CUDA tensor) for density x (n, n), spectrum
+        coefficients Ie (J, float64) and measured intensity imea (np, prjWidth)."""
+        import torch
+        out = torch.empty(1, dtype=torch.float64, device=x.device) if out is None else out
+        px, pI, pm = self._args(x, Ie, imea)
+        check(lib().ctprj_bhc_forward(self._m, px, pI, pm, _dptr(out, 1, torch.float64),
+                                      1 if save else 0, _stream_handle(stream, self.projector.device)))
+        return out
+
+    def terms(self, sino, Ie, imea, save=True, out=None, stream=None):
+        """The same likelihood from a plain sinogram (unfused path)."""
+        import torch
+        out = torch.empty(1, dtype=torch.float64, device=sino.device) if out is None else out
+        pr = self.projector
+        _, pI, pm = self._args(None, Ie, imea)
+        check(lib().ctprj_bhc_terms(self._m, _dev_ptr(sino, pr.sino_shape, pr.device), pI, pm,
+                                    _dptr(out, 1, torch.float64), 1 if save else 0,
+                                    _stream_handle(stream, pr.device)))
+        return out
+
+    def backward(self, x=None, Ie=None, imea=None, grad_x=True, grad_Ie=True, stream=None):
+        """(df/dx as (n, n) float32, df/dIe as (J,) float64); either may be None
+        when not requested.  Recomputes the forward when it saved no state."""
+        import torch
+        pr = self.projector
+        dev = "cuda:%d" % pr.device
+        gx = torch.empty(pr.img_shape, dtype=torch.float32, device=dev) if grad_x else None
+        gI = torch.empty(self.J, dtype=torch.float64, device=dev) if grad_Ie else None
+        px, pI, pm = self._args(x, Ie, imea)
+        check(lib().ctprj_bhc_backward(self._m, px, pI, pm,
+                                       _dev_ptr(gx, pr.img_shape, pr.device) if gx is not None else None,
+                                       _dptr(gI, self.J, torch.float64) if gI is not None else None,
+                                       _stream_handle(stream, pr.device)))
+        return gx, gI

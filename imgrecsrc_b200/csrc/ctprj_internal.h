@@ -53,12 +53,26 @@ struct Geo {
     float effRate;
 };
 
+// Polychromatic epilogue of the fused forward pass (bhc.cu).
+struct BhcArgs {
+    const double *tab;        // spline table, J * kSplStride doubles
+    const double *Ie;         // spectrum coefficients, J doubles
+    int J;
+    double Ts;                // pixel size: s = Ts * (A x)
+    const float *imea;        // measured intensity / I0 per ray (np * prjWidth)
+    float *s_out, *r_out, *w_out;   // per-ray s, 1 - m/BL, (1 - m/BL) dBL/ds; NULL: not kept
+    double *part;             // per-block partial sums of the Poisson terms
+};
+
+enum { kModePlain = 0, kModeCount = 1, kModeBhc = 2 };
+
 struct FwdParams {
     Geo g;
     int nb, k0, nk;           // base views, first ray, rays per base view
     int zero_col0;            // even prjWidth: detector 0 written as zero
     const FwdView *view;
     const DetEntry *det;
+    BhcArgs bhc;
 };
 
 struct BwdParams {
@@ -66,7 +80,7 @@ struct BwdParams {
     int nv;                   // base views looped over
     int tiles_side;
     int zero_axes;            // even n: row 0 and column 0 written as zero
-    float fbp_scale;          // FBP: PI_f/np/dSize/dSize, else 1
+    float scale;              // output scale: FBP PI_f/np/dSize^2, BHC gradient Ts, else 1
     const BwdView *view;
     const DetEntry *det;
 };
@@ -98,7 +112,12 @@ int cuda_error(cudaError_t e, const char *what);
 int launch_transpose(const float *src, float *dst, int n, cudaStream_t s);
 int launch_forward(const ctprj_plan *p, const float *img, const float *imgT, float *sino,
                    unsigned long long *counter, cudaStream_t s);
+// fused forward projection + polychromatic epilogue; returns the number of
+// per-block partials written to a.part
+int launch_forward_bhc(const ctprj_plan *p, const float *img, const float *imgT,
+                       const BhcArgs &a, int *nparts, cudaStream_t s);
+int forward_blocks(const ctprj_plan *p);
 int launch_backward(const ctprj_plan *p, const float *sino, float *img, int fbp,
-                    unsigned long long *counter, cudaStream_t s);
+                    unsigned long long *counter, cudaStream_t s, float scale = 1.0f);
 
 }  // namespace ctprj

@@ -121,6 +121,48 @@ int ctprj_fbp(ctprj_plan *plan, const float *d_sino, float *d_img, void *stream)
  * visit (ray-pixel updates per call), counted on the device. */
 int ctprj_count_updates(ctprj_plan *plan, long long *fwd, long long *bwd, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Polychromatic beam-hardening model (bhc/Spline.m b1Iout, bhc/poissLAlpha.m,
+ * bhc/poissLI.m) on a plan.  Per ray i: s_i = Ts (A x)_i, the degree-1
+ * B-spline spectrum model BL_i = sum_j Ie_j b_j(s_i) over J basis functions
+ * on the J + 2 mass-attenuation nodes kappa (bhc/Spline.m:122-203), and the
+ * Poisson negative log-likelihood of the measured intensity m_i (counts / I0):
+ *   f = sum_i BL_i - m_i - m_i log(BL_i / m_i)   (0 log 0 := 0),
+ * with gradients df/dx = Ts A^T [(1 - m/BL) dBL/ds] and
+ * df/dIe_j = sum_i b_j(s_i) (1 - m_i/BL_i).  Spline arithmetic and every
+ * reduction are FP64; projections FP32.  One model per stream at a time.
+ * ---------------------------------------------------------------------- */
+
+typedef struct ctprj_bhc ctprj_bhc;
+
+/* J in [1, 32]; kappa_nodes: J + 2 increasing positive nodes (cm^2/g);
+ * Ts > 0: pixel size (cm).  Allocates per-ray state (3 floats per ray). */
+int ctprj_bhc_create(ctprj_plan *plan, int J, const double *kappa_nodes, double Ts,
+                     ctprj_bhc **model);
+void ctprj_bhc_destroy(ctprj_bhc *model);
+
+/* Fused forward: projection and per-ray spline epilogue in one kernel; the
+ * likelihood f is reduced in FP64 into d_f (1 double, device).  d_x: n*n
+ * float; d_Ie: J doubles; d_imea: np*prjWidth floats.  save != 0 keeps the
+ * per-ray state for ctprj_bhc_backward; save == 0 writes nothing per ray. */
+int ctprj_bhc_forward(ctprj_bhc *model, const float *d_x, const double *d_Ie,
+                      const float *d_imea, double *d_f, int save, void *stream);
+
+/* Gradients of the last forward: d_gx (n*n floats) and d_gIe (J doubles,
+ * FP64); either may be NULL.  When the last forward did not save its state,
+ * the fused forward is recomputed from d_x, d_Ie, d_imea first. */
+int ctprj_bhc_backward(ctprj_bhc *model, const float *d_x, const double *d_Ie,
+                       const float *d_imea, float *d_gx, double *d_gIe, void *stream);
+
+/* The same per-ray terms as the fused epilogue, evaluated by a separate kernel
+ * over a sinogram d_sino from ctprj_forward (the unfused path). */
+int ctprj_bhc_terms(ctprj_bhc *model, const float *d_sino, const double *d_Ie,
+                    const float *d_imea, double *d_f, int save, void *stream);
+
+/* Device pointers of the saved per-ray state: s_i, 1 - m_i/BL_i and
+ * (1 - m_i/BL_i) dBL/ds (np*prjWidth floats each). */
+int ctprj_bhc_state(ctprj_bhc *model, const float **d_s, const float **d_r, const float **d_w);
+
 /* Static description of a status code, and the message of the last failure on
  * the calling thread. */
 const char *ctprj_error_string(int status);

@@ -109,11 +109,15 @@ def test_adjoint_dot_product(name):
 
 @pytest.mark.parametrize("name", ["par256", "fan512", "fan_odd"])
 def test_update_counts_match_oracle(name):
+    # A footprint weight that is exactly zero in FP64 at the edge of a ray's
+    # pixel range can round to a tiny nonzero value in FP32 and vice versa
+    # (axis-aligned parallel views put many pixels exactly on that edge), so
+    # the device count agrees with the oracle's to 1e-4, not exactly.
     g = CONFIGS[name]
     f, b = ct.Projector(g).count_updates()
     fo, bo = oracle.forward_nnz(g), oracle.backward_nnz(g)
-    assert abs(f - fo) <= 1e-5 * fo
-    assert abs(b - bo) <= 1e-5 * bo
+    assert abs(f - fo) <= 1e-4 * fo
+    assert abs(b - bo) <= 1e-4 * bo
 
 
 def test_mex_gateway_mirror_matches_device_path():
