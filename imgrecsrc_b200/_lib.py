@@ -18,6 +18,13 @@ class CtprjError(RuntimeError):
         self.status = status
 
 
+class ParConf(ctypes.Structure):
+    """parConf of include/parprj.h (prj/parPrj.h:9-16)."""
+    _fields_ = [("bw", ctypes.c_double), ("nc", ctypes.c_int), ("nr", ctypes.c_int),
+                ("np", ctypes.c_int), ("prjWidth", ctypes.c_int),
+                ("theta", ctypes.POINTER(ctypes.c_double)), ("fwd", ctypes.c_int)]
+
+
 class Geometry(ctypes.Structure):
     """struct ctprj_geometry -- the reference's projector configuration
     (prj/prj.h:42-57): n, prjWidth, np, prjFull, dSize, effectiveRate, d."""
@@ -70,7 +77,11 @@ def lib():
         "ctprj_bhc_forward": ([VP, VP, VP, VP, VP, ctypes.c_int, VP], ctypes.c_int),
         "ctprj_bhc_backward": ([VP, VP, VP, VP, VP, VP, VP], ctypes.c_int),
         "ctprj_bhc_terms": ([VP, VP, VP, VP, VP, ctypes.c_int, VP], ctypes.c_int),
+        "ctprj_bhc_basis": ([VP, VP, VP, VP], ctypes.c_int),
         "ctprj_bhc_state": ([VP, ctypes.POINTER(VP), ctypes.POINTER(VP), ctypes.POINTER(VP)], ctypes.c_int),
+        "parPrjConf": ([VP, VP, VP, ctypes.POINTER(ParConf), ctypes.c_size_t], ctypes.c_int),
+        "parPrjThread": ([], ctypes.c_int),
+        "parPrjRun": ([], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

@@ -14,7 +14,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import BWD_BIT, FBP_BIT, FWD_BIT, check, lib
+from ._lib import BWD_BIT, FBP_BIT, FWD_BIT, ParConf, check, lib
 
 _conf = None
 
@@ -60,3 +60,33 @@ def gpuPrj(x, conf, cmd):
         return img.astype(np.float64).ravel(order="F")
     L.showSetup()
     return None
+
+
+def mParPrj(x, maskIdx, conf, cmd):
+    """The MEX function mParPrj(x, maskIdx, conf, cmd) of prj/mParPrj.c:26-74:
+    the double-precision parallel-beam operator over the angles conf.theta
+    (degrees) and the 0-based column-major pixel indices maskIdx of an
+    conf.nr x conf.nc image, beam width conf.bw, conf.prjWidth detectors.
+    'forward' maps one value per mask entry to np*prjWidth values; any other
+    command is the backprojection.  Returns a float64 vector."""
+    theta = np.ascontiguousarray(_field(conf, "theta"), np.float64).ravel()
+    mask = np.ascontiguousarray(maskIdx, np.float64).ravel()
+    x = np.ascontiguousarray(x, np.float64).ravel()
+    W = int(_field(conf, "prjWidth"))
+    fwd = cmd == "forward"
+    pc = ParConf(float(_field(conf, "bw")), int(_field(conf, "nc")), int(_field(conf, "nr")),
+                 theta.size, W, theta.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                 1 if fwd else 0)
+    if fwd:
+        img, prj = x, np.zeros(theta.size * W, np.float64)     # mxCreateDoubleMatrix zeros
+        out = prj
+    else:
+        if x.size != theta.size * W:
+            raise ValueError("expected %d sinogram values" % (theta.size * W))
+        img, prj = np.zeros(mask.size, np.float64), x.copy()
+        out = img
+    L = lib()
+    check(L.parPrjConf(img.ctypes.data, prj.ctypes.data, mask.ctypes.data, ctypes.byref(pc),
+                       mask.size))
+    check(L.parPrjThread())
+    return out

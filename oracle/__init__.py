@@ -58,6 +58,15 @@ def build_ref(ref_prj_dir="/root/reference/prj"):
     return True
 
 
+def build_gateways(ref_prj_dir="/root/reference/prj"):
+    """The reference's own MEX gateways compiled against the engine library
+    (oracle/Makefile target `gateways`), for the boundary tests."""
+    if not os.path.isdir(ref_prj_dir):
+        return False
+    subprocess.run(["make", "-s", "-C", HERE, "gateways", "REF=" + ref_prj_dir], check=True)
+    return True
+
+
 def _load(name, builder):
     with _lock:
         if name in _libs:
