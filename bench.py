@@ -37,6 +37,10 @@ WORKLOAD = dict(workload="fan-beam fwd+backprojection 2048^2, 1440 views/[0,2pi)
 CPU_SAMPLE = dict(n=1024, prjWidth=1024, np=1440, prjFull=1440, dSize=1.0, effectiveRate=1.0,
                   d=4096.0)
 L2_FLUSH_BYTES = 512 << 20   # > 126 MB L2
+# polychromatic (BHC) gradient iteration on the same geometry: two-material
+# phantom (0 / 2.7 / 7.8 g/cm^3), J = 30 b1 coefficients on kappa log-spaced over
+# [1e-2, 1e2] cm^2/g, Poisson counts at I0 = 1e5 per ray, 2 cm field of view
+BHC = dict(J=30, I0=1e5, fov_cm=2.0)
 
 
 def geometry_tuple(w):
@@ -247,6 +251,8 @@ def our_arm(args):
     achieved = kbytes / (kms * 1e-3) / 1e9
     traffic = PROFILED_TRAFFIC.get("k_backward" if bwd_ms >= fwd_ms else "k_forward")
 
+    bhc_line = bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
+
     # end to end through the reference-facing C ABI: setup() once, then per
     # step gpuPrj(FWD) and gpuPrj(BWD) on pinned host buffers (every call
     # copies its input to the device and its result back, as the reference does)
@@ -293,6 +299,7 @@ def our_arm(args):
                 "ms_per_step": e2e_t * 1e3},
         "gpu_launches": 3 * args.steps,
         "clocks": clk,
+        "bhc": bhc_line,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         v, t, info = cpu_reference_run(1, 0)
@@ -302,6 +309,75 @@ def our_arm(args):
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def bhc_leg(ct, g, pr, flush, stream, steps):
+    """BHC gradient iterations per second: the fused forward (projection with
+    the spline epilogue) + adjoint, against the plain FP32 projector path in
+    the reference's call structure (bhc/beamhardenSpline.m:382-447: Phi(alpha),
+    unfused polyIout + poissLAlpha terms, Phit; then Phi(alpha) again, the
+    materialised rays x J basis matrix and A^T (1 - m/Ir) of poissLI) and
+    against a minimal plain path (one projection, unfused terms, same adjoint).
+    Each iteration yields f (FP64), df/dx and df/dIe."""
+    import torch
+
+    from imgrecsrc_b200 import bhc, phantom
+    J, I0 = BHC["J"], BHC["I0"]
+    Ts = BHC["fov_cm"] / g.n
+    x = torch.from_numpy(phantom.two_material_phantom(g.n, seed=2)).cuda()
+    nodes = bhc.kappa_nodes(J)
+    Ie = torch.from_numpy(phantom.spectrum_bump(J, seed=2)).cuda()
+    model = bhc.BHCModel(pr, nodes, Ts)
+    sino = pr.forward(x)
+    A = model.basis(sino)
+    BL = (A @ Ie).reshape(g.np, g.prjWidth)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    imea = (torch.poisson(I0 * BL, generator=gen) / I0).float().contiguous()
+    del A, BL
+
+    def fused():
+        model.forward(x, Ie, imea, save=True)
+        return model.backward()
+
+    def plain_ref():
+        s1 = pr.forward(x)
+        model.terms(s1, Ie, imea, save=True)
+        gx, _ = model.backward(grad_Ie=False)
+        s2 = pr.forward(x)
+        Am = model.basis(s2)
+        gI = Am.t() @ (1 - imea.double().ravel() / (Am @ Ie))
+        return gx, gI
+
+    def plain_min():
+        s1 = pr.forward(x)
+        model.terms(s1, Ie, imea, save=True)
+        return model.backward()
+
+    out = {"workload": "fan 2048^2, 1440 views, 2048 bins, d=8192 px; two-material phantom; "
+                       "J=30 b1 spectrum on [1e-2,1e2] cm^2/g; Poisson counts I0=1e5; Ts=%g cm" % Ts,
+           "iteration": "f (FP64) + df/dx + df/dIe"}
+    for name, fn in (("fused", fused), ("plain", plain_ref), ("plain_min", plain_min)):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ms = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        ms /= steps
+        out[name + "_ms"] = ms
+        out[name + "_grad_iter_per_s"] = 1e3 / ms
+    out["speedup_vs_plain"] = out["plain_ms"] / out["fused_ms"]
+    out["speedup_vs_plain_min"] = out["plain_min_ms"] / out["fused_ms"]
+    out["fused_launches_per_iter"] = 6
+    model.close()
+    return out
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from the ncu

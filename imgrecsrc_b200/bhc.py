@@ -87,6 +87,16 @@ class BHCModel:
                                     _stream_handle(stream, pr.device)))
         return out
 
+    def basis(self, sino, out=None, stream=None):
+        """The (rays, J) FP64 basis matrix b_j(Ts * sino_i)."""
+        import torch
+        pr = self.projector
+        out = torch.empty(self.nrays, self.J, dtype=torch.float64, device=sino.device) if out is None else out
+        check(lib().ctprj_bhc_basis(self._m, _dev_ptr(sino, pr.sino_shape, pr.device),
+                                    _dptr(out, self.nrays * self.J, torch.float64),
+                                    _stream_handle(stream, pr.device)))
+        return out
+
     def backward(self, x=None, Ie=None, imea=None, grad_x=True, grad_Ie=True, stream=None):
         """(df/dx as (n, n) float32, df/dIe as (J,) float64); either may be None
         when not requested.  Recomputes the forward when it saved no state."""

@@ -222,6 +222,17 @@ static int build_plan(const ctprj_geometry *geom, int device, ctprj_plan **out)
         free_plan(p);
         return st;
     }
+    // backprojection kernel: staged tiles sized to the widest tile shadow of
+    // this geometry, or the unstaged kernel when a shadow exceeds 64 detectors
+    // or CTPRJ_BWD_KERNEL=direct asks for it (kept for comparison)
+    int span = 0;
+    if ((st = backward_max_span(p, &span))) {
+        free_plan(p);
+        return st;
+    }
+    const char *bk = getenv("CTPRJ_BWD_KERNEL");
+    p->bwd_seg = span < 32 ? 32 : (span < 64 ? 64 : 0);
+    if (bk && strcmp(bk, "direct") == 0) p->bwd_seg = 0;
     *out = p;
     return CTPRJ_OK;
 }

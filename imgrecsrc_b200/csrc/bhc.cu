@@ -128,6 +128,34 @@ k_bhc_terms(const float *__restrict__ sino, long long nrays, BhcArgs a)
     if (threadIdx.x == 0) a.part[blockIdx.x] = t;
 }
 
+// The rays x J basis matrix A[i][j] = b_j(Ts * sino_i) in FP64 (Spline.b1Iout
+// with I empty, bhc/Spline.m:143, :168), materialised as the reference's
+// spectrum step does (bhc/beamhardenSpline.m:447).
+__global__ void __launch_bounds__(256)
+k_bhc_basis(const float *__restrict__ sino, long long nrays, const double *__restrict__ tab_g,
+            int J, double Ts, double *__restrict__ A)
+{
+    __shared__ double tab[kMaxJ * kSplStride];
+    for (int i = threadIdx.x; i < J * kSplStride; i += blockDim.x) tab[i] = tab_g[i];
+    __syncthreads();
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double si = Ts * (double)sino[i];
+        const double is2 = 1.0 / (si * si), as = fabs(si);
+        double eL = exp(-tab[0] * si), eC = exp(-tab[1] * si);
+        double *row = A + (size_t)i * J;
+        for (int j = 0; j < J; ++j) {
+            const double *t = tab + j * kSplStride;
+            const double eR = exp(-t[2] * si);
+            double bj = ((eC - eR) * t[4] - (eL - eC) * t[3]) * is2;
+            if (as < t[9]) bj = fma(fma(fma(t[8], si, t[7]), si, t[6]), si, t[5]);
+            row[j] = bj;
+            eL = eC;
+            eC = eR;
+        }
+    }
+}
+
 // out[c] = sum over b < nrows of part[b * ncols + c], in a fixed order (FP64)
 __global__ void k_sum_columns(const double *__restrict__ part, int nrows, int ncols,
                               double *__restrict__ out)
@@ -341,6 +369,16 @@ extern "C" int ctprj_bhc_backward(ctprj_bhc *m, const float *d_x, const double *
     }
     m->saved = 1;
     return CTPRJ_OK;
+}
+
+extern "C" int ctprj_bhc_basis(ctprj_bhc *m, const float *d_sino, double *d_A, void *stream)
+{
+    if (!m || !d_sino || !d_A) return set_error(CTPRJ_EINVAL, "NULL argument");
+    PlanDevice pd(m->plan->device);
+    const long long nr = (long long)m->plan->g.np * m->plan->g.W;
+    k_bhc_basis<<<4 * spectrum_blocks(), 256, 0, (cudaStream_t)stream>>>(d_sino, nr, m->d_tab, m->J,
+                                                                         m->Ts, d_A);
+    return cuda_error(cudaGetLastError(), "basis matrix");
 }
 
 extern "C" int ctprj_bhc_state(ctprj_bhc *m, const float **d_s, const float **d_r, const float **d_w)

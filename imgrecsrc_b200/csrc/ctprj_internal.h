@@ -93,6 +93,7 @@ struct ctprj_plan {
     ctprj::Geo g;
     int nb, k0, nk;           // forward ray set (prj/cpuPrj.c:326-332, :469-475)
     int nv;                   // backward view count
+    int bwd_seg;              // staged detectors per view and tile (32, 64), 0: unstaged
     ctprj::FwdView *d_fview;
     ctprj::BwdView *d_bview;
     ctprj::DetEntry *d_det;
@@ -117,6 +118,7 @@ int launch_forward(const ctprj_plan *p, const float *img, const float *imgT, flo
 int launch_forward_bhc(const ctprj_plan *p, const float *img, const float *imgT,
                        const BhcArgs &a, int *nparts, cudaStream_t s);
 int forward_blocks(const ctprj_plan *p);
+int backward_max_span(const ctprj_plan *p, int *max_span);
 int launch_backward(const ctprj_plan *p, const float *sino, float *img, int fbp,
                     unsigned long long *counter, cudaStream_t s, float scale = 1.0f);
 

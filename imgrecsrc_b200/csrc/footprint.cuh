@@ -49,4 +49,53 @@ __device__ __forceinline__ float footprint_weight(float dist, float bw, const Fo
     return f.h * (trap_cdf(hb - dist, f) - trap_cdf(-hb - dist, f));
 }
 
+// The same weight with every clamp done by the FMA pipe's saturation to [0, 1]
+// instead of min/max on the ALU pipe.  With P = sat((u + b2)/w),
+// R = sat((u - b1)/w) and Q = sat((u + b1)/(2 b1)) the cumulative area is
+//   G(u) = w/2 (P^2 - R^2) + 2 b1 Q + w R,
+// and the coefficients below fold in the plateau height.  A ramp width or
+// shoulder width of zero gets a huge finite reciprocal whose saturated terms
+// are multiplied by that zero width, so axis-aligned and diagonal rays need no
+// branch.  The rounding of (u + b2)/w is bounded by b2 ulp(1) / w and is scaled
+// back by w, so the absolute error stays below ~1e-7 for any ramp width.
+struct FootprintSat {
+    float hw;    // h w / 2
+    float tb;    // h 2 b1
+    float hwr;   // h w
+    float iw;    // 1 / w
+    float c1;    // b2 / w
+    float c2;    // -b1 / w
+    float i2b;   // 1 / (2 b1)
+};
+
+__host__ __device__ __forceinline__ FootprintSat make_footprint_sat(float c, float s)
+{
+    const Footprint f = make_footprint(c, s);
+    FootprintSat q;
+    const float w = f.w > 1e-30f ? f.w : 1e-30f;
+    const float tb = 2.0f * f.b1 > 1e-30f ? 2.0f * f.b1 : 1e-30f;
+    q.iw = 1.0f / w;
+    q.c1 = f.b2 * q.iw;
+    q.c2 = -f.b1 * q.iw;
+    q.i2b = 1.0f / tb;
+    q.hw = f.h * 0.5f * f.w;
+    q.tb = f.h * 2.0f * f.b1;
+    q.hwr = f.h * f.w;
+    return q;
+}
+
+__device__ __forceinline__ float trap_cdf_sat(float u, const FootprintSat &q)
+{
+    const float P = __saturatef(fmaf(u, q.iw, q.c1));
+    const float R = __saturatef(fmaf(u, q.iw, q.c2));
+    const float Q = __saturatef(fmaf(u, q.i2b, 0.5f));
+    return fmaf(q.hw, fmaf(P, P, -R * R), fmaf(q.tb, Q, q.hwr * R));
+}
+
+// footprint weight for a beam of half-width hb
+__device__ __forceinline__ float footprint_weight_sat(float dist, float hb, const FootprintSat &q)
+{
+    return trap_cdf_sat(hb - dist, q) - trap_cdf_sat(-hb - dist, q);
+}
+
 }  // namespace ctprj

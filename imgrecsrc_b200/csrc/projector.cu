@@ -31,6 +31,10 @@
 namespace ctprj {
 
 constexpr int kFwdThreads = 128;
+// a forward block is kFwdViews adjacent base views x 32 adjacent rays, one view
+// per warp: the warps march over nearly the same image lines at the same time,
+// so the rows they gather are shared in L1
+constexpr int kFwdViews = kFwdThreads / 32;
 constexpr int kBwdTile = 16;   // 16 x 16 octant pixels per block
 
 // --------------------------------------------------------------- transpose
@@ -97,8 +101,8 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
           float *__restrict__ sino, unsigned long long *__restrict__ counter)
 {
     const Geo &g = p.g;
-    const int b = blockIdx.x;
-    const int r = blockIdx.y * blockDim.x + threadIdx.x;
+    const int b = blockIdx.x * kFwdViews + (int)(threadIdx.x >> 5);
+    const int r = blockIdx.y * 32 + (int)(threadIdx.x & 31);
     double fsum = 0.0;            // polychromatic mode: this thread's Poisson terms
     const double *tab = nullptr, *Ie = nullptr;
     if constexpr (MODE == kModeBhc) {
@@ -110,13 +114,13 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
         Ie = sm + kMaxJ * kSplStride;
     }
     // detector 0 of an even-width sinogram: no ray, zero projection
-    if (MODE != kModeCount && p.zero_col0 && b == 0 && blockIdx.y == 0)
+    if (MODE != kModeCount && p.zero_col0 && blockIdx.x == 0 && blockIdx.y == 0)
         for (int v = threadIdx.x; v < g.np; v += blockDim.x) {
             if constexpr (MODE == kModeBhc) fsum += bhc_entry(p.bhc, tab, Ie, 0.0f, (size_t)v * g.W);
             else sino[(size_t)v * g.W] = 0.0f;
         }
 
-    if (r < p.nk) {
+    if (b < p.nb && r < p.nk) {
         const int k = p.k0 + r;
         const double cT = p.view[b].c, sT = p.view[b].s;
         const DetEntry de = p.det[k];
@@ -155,8 +159,8 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
         }
         const float Alf = (float)Al, Slf = (float)Sl, Arf = (float)Ar, Srf = (float)Sr;
         const float cRf = (float)cR, cTf = (float)cT, sTf = (float)sT;
-        const float dbw = FAN ? sTf * kbw : 0.0f;
-        const Footprint fp = make_footprint(cRf, (float)sR);
+        const float dhb = FAN ? 0.5f * sTf * kbw : 0.0f;   // half beam width step per pixel
+        const FootprintSat fp = make_footprint_sat(cRf, (float)sR);
 
         const int N = g.n, half = g.half, h2 = g.h2;
         float S[8];
@@ -164,29 +168,34 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
         for (int j = 0; j < 8; ++j) S[j] = 0.0f;
         unsigned long long nz = 0;
 
-        for (int y = half; y >= -half; --y) {
+        // rows y and -y of the image and of its transpose, centred on x = 0:
+        // a0[x] = I(x, y), a0[-x] = I(-x, y), a1[+-x] = I(+-x, -y),
+        // t0[x] = I(y, x), t0[-x] = I(y, -x), t1[+-x] = I(-y, +-x);
+        // stepped with the row
+        const float *a0 = img + (size_t)(half + h2) * N + h2;
+        const float *a1 = img + (size_t)(h2 - half) * N + h2;
+        const float *t0 = imgT + (size_t)(half + h2) * N + h2;
+        const float *t1 = imgT + (size_t)(h2 - half) * N + h2;
+        for (int y = half; y >= -half; --y, a0 -= N, a1 += N, t0 -= N, t1 += N) {
             const float yf = (float)y;
             const float xl = fmaf(-yf, Slf, Alf), xr = fmaf(-yf, Srf, Arf);
-            int x0 = (int)roundf(fmaxf(xl, (float)(-half - 1)));
-            int x1 = (int)roundf(fminf(xr, (float)(half + 1)));
+            // nearest pixel to each edge; exact half-way ties (where the
+            // reference rounds away from zero) only decide pixels whose
+            // footprint just touches the beam edge, with weight zero
+            int x0 = __float2int_rn(fmaxf(xl, (float)(-half - 1)));
+            int x1 = __float2int_rn(fminf(xr, (float)(half + 1)));
             x0 = max(x0, -half);
             x1 = min(x1, half);
             if (x0 > x1) continue;
             // distance of pixel (x0, y) from the ray, in FP64 then rounded
             const float r0 = (float)fma((double)x0, cR, fma((double)y, sR, -off));
-            const float bw0 = FAN ? fmaf(fmaf((float)x0, sTf, -yf * cTf), kbw, bwc) : g.beamWidthF;
-            // rows y and -y of the image and of its transpose, centred on x = 0:
-            // a0[x] = I(x, y), a0[-x] = I(-x, y), a1[+-x] = I(+-x, -y),
-            // t0[x] = I(y, x), t0[-x] = I(y, -x), t1[+-x] = I(-y, +-x)
-            const float *a0 = img + (size_t)(y + h2) * N + h2;
-            const float *a1 = img + (size_t)(h2 - y) * N + h2;
-            const float *t0 = imgT + (size_t)(y + h2) * N + h2;
-            const float *t1 = imgT + (size_t)(h2 - y) * N + h2;
+            const float hb0 = FAN ? 0.5f * fmaf(fmaf((float)x0, sTf, -yf * cTf), kbw, bwc)
+                                  : 0.5f * g.beamWidthF;
             for (int x = x0; x <= x1; ++x) {
                 const float jf = (float)(x - x0);
                 const float dist = fmaf(jf, cRf, r0);
-                const float bw = FAN ? fmaf(jf, dbw, bw0) : bw0;
-                const float w = footprint_weight(dist, bw, fp);
+                const float hb = FAN ? fmaf(jf, dhb, hb0) : hb0;
+                const float w = footprint_weight_sat(dist, hb, fp);
                 if (MODE == kModeCount) {
                     nz += (w != 0.0f);
                     continue;
@@ -208,6 +217,11 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
         // coincide (the central detector) the second write is the one kept.
         const int pC = g.pC;
         unsigned long long entries = 0;
+        // polychromatic mode: the entries this ray sum feeds, gathered first so
+        // that one copy of the FP64 epilogue serves them all
+        float eval[16];
+        int eidx[16];
+        int ne = 0;
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
             const int v = p.view[b].out[j];
@@ -219,17 +233,21 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
                 entries += (!FAN && det2 != det) ? 2 : 1;
             } else if constexpr (MODE == kModeBhc) {
                 if (FAN) {
-                    fsum += bhc_entry(p.bhc, tab, Ie, S[j] / g.effRate, row + det);
+                    eval[ne] = S[j] / g.effRate; eidx[ne++] = (int)(row + det);
                 } else if (det2 != det) {
-                    fsum += bhc_entry(p.bhc, tab, Ie, S[j] / g.effRate, row + det);
-                    fsum += bhc_entry(p.bhc, tab, Ie, S[j ^ 2] / g.effRate, row + det2);
+                    eval[ne] = S[j] / g.effRate; eidx[ne++] = (int)(row + det);
+                    eval[ne] = S[j ^ 2] / g.effRate; eidx[ne++] = (int)(row + det2);
                 } else {
-                    fsum += bhc_entry(p.bhc, tab, Ie, S[j ^ 2] / g.effRate, row + det);
+                    eval[ne] = S[j ^ 2] / g.effRate; eidx[ne++] = (int)(row + det);
                 }
             } else {
                 sino[row + det] = S[j] / g.effRate;
                 if (!FAN) sino[row + det2] = S[j ^ 2] / g.effRate;
             }
+        }
+        if constexpr (MODE == kModeBhc) {
+#pragma unroll 1
+            for (int e = 0; e < ne; ++e) fsum += bhc_entry(p.bhc, tab, Ie, eval[e], (size_t)eidx[e]);
         }
         if (MODE == kModeCount && nz * entries) atomicAdd(counter, nz * entries);
     }
@@ -257,7 +275,7 @@ static FwdParams fwd_params(const ctprj_plan *pl)
 
 static dim3 fwd_grid(const ctprj_plan *pl)
 {
-    return dim3(pl->nb, (pl->nk + kFwdThreads - 1) / kFwdThreads);
+    return dim3((pl->nb + kFwdViews - 1) / kFwdViews, (pl->nk + 31) / 32);
 }
 
 int forward_blocks(const ctprj_plan *pl)
@@ -312,106 +330,97 @@ __device__ __forceinline__ void image_of(int j, int x, int y, int &gx, int &gy)
     }
 }
 
+// One base view of the pixel-driven backprojection for octant pixel (x, y):
+// the detectors under the pixel's shadow, one footprint weight each, serving
+// the eight symmetric images (prj/cpuPrj.c:213-300).  Everything is read from
+// global memory (L1); used by k_backward_direct and, for views whose tile
+// shadow exceeds the staging capacity, by k_backward_tiled.
 template <bool FAN, bool COUNT, bool FBP>
-__global__ void __launch_bounds__(kBwdTile * kBwdTile)
-k_backward(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img,
-           unsigned long long *__restrict__ counter)
+__device__ __forceinline__ void bwd_view_direct(const BwdParams &p, const float *__restrict__ sino,
+                                                int i, int x, int y, int nimg, float (&S)[8],
+                                                unsigned long long &nz)
 {
     const Geo &g = p.g;
-    if (!COUNT && p.zero_axes && blockIdx.x == 0)
-        for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
-            img[i] = 0.0f;
-            img[(size_t)i * g.n] = 0.0f;
-        }
-    // triangular tile number -> tile (tx, ty), ty <= tx
-    const int tile = blockIdx.x;
-    int tx = (int)((sqrtf(8.0f * (float)tile + 1.0f) - 1.0f) * 0.5f);
-    while ((tx + 1) * (tx + 2) / 2 <= tile) ++tx;
-    while (tx * (tx + 1) / 2 > tile) --tx;
-    const int ty = tile - tx * (tx + 1) / 2;
-    const int x = tx * kBwdTile + (int)(threadIdx.x % kBwdTile);
-    const int y = ty * kBwdTile + (int)(threadIdx.x / kBwdTile);
-    if (x > g.half || y > x) return;
-
-    const int nimg = (y == 0 || y == x) ? 4 : 8;
-    const double xd = x, yd = y;
-    const float xf = (float)x, yf = (float)y;
     const int dmax = (g.W - 1) / 2, pC = g.pC;
     const float dSf = (float)g.dSize;
-    float S[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) S[j] = 0.0f;
-    unsigned long long nz = 0;
-
-    for (int i = 0; i < p.nv; ++i) {
-        const BwdView &bv = p.view[i];
-        const double cT = bv.c, sT = bv.s;
-        const float cTf = bv.cf, sTf = bv.sf;
-        const double u = fma(xd, cT, yd * sT);    // along the detector
-        float tlo, thi, qe = 0.0f;
-        double v = 0.0;
+    const double xd = x, yd = y;
+    const float xf = (float)x, yf = (float)y;
+    const BwdView &bv = p.view[i];
+    const double cT = bv.c, sT = bv.s;
+    const float cTf = bv.cf, sTf = bv.sf;
+    const double u = fma(xd, cT, yd * sT);    // along the detector
+    float tlo, thi, qe = 0.0f;
+    double v = 0.0;
+    if (FAN) {
+        // shadow of the pixel's corners on the virtual detector
+        // (prj/cpuPrj.c:218-244)
+        v = fma(yd, cT, -xd * sT);
+        qe = (float)(g.d - v);
+        const float ocm = fmaf(xf - 0.5f, cTf, (yf - 0.5f) * sTf);
+        const float qem = fmaf(xf - 0.5f, sTf, -(yf - 0.5f) * cTf) + g.dF;
+        const float t0 = g.dF * ocm / qem;
+        const float t1 = g.dF * (ocm + cTf) / (qem + sTf);
+        const float t2 = g.dF * (ocm + cTf + sTf) / (qem + sTf - cTf);
+        const float t3 = g.dF * (ocm + sTf) / (qem - cTf);
+        tlo = fminf(fminf(t0, t1), fminf(t2, t3));
+        thi = fmaxf(fmaxf(t0, t1), fmaxf(t2, t3));
+    } else {
+        const float hw = 0.5f * (fabsf(cTf) + fabsf(sTf));
+        const float uf = (float)u;
+        tlo = uf - hw;
+        thi = uf + hw;
+    }
+    int dl = (int)roundf(fmaxf(tlo / dSf, (float)(-dmax - 1)));
+    int dr = (int)roundf(fminf(thi / dSf, (float)(dmax + 1)));
+    dl = max(dl, -dmax);
+    dr = min(dr, dmax);
+    Footprint pfp;
+    if (!FAN) {
+        pfp.h = bv.h; pfp.b1 = bv.b1; pfp.b2 = bv.b2; pfp.w = bv.w; pfp.iw2 = bv.iw2;
+    }
+    for (int dt = dl; dt <= dr; ++dt) {
+        const DetEntry &de = p.det[dt + pC];
+        float w;
         if (FAN) {
-            // shadow of the pixel's corners on the virtual detector
-            // (prj/cpuPrj.c:218-244)
-            v = fma(yd, cT, -xd * sT);
-            qe = (float)(g.d - v);
-            const float ocm = fmaf(xf - 0.5f, cTf, (yf - 0.5f) * sTf);
-            const float qem = fmaf(xf - 0.5f, sTf, -(yf - 0.5f) * cTf) + g.dF;
-            const float t0 = g.dF * ocm / qem;
-            const float t1 = g.dF * (ocm + cTf) / (qem + sTf);
-            const float t2 = g.dF * (ocm + cTf + sTf) / (qem + sTf - cTf);
-            const float t3 = g.dF * (ocm + sTf) / (qem - cTf);
-            tlo = fminf(fminf(t0, t1), fminf(t2, t3));
-            thi = fmaxf(fmaxf(t0, t1), fmaxf(t2, t3));
+            // distance from the detector's ray: cos B (u - t) + sin B v
+            const float dist = (float)fma(de.cB, u - de.t, de.sB * v);
+            const float cR = fmaf(de.cBf, cTf, -de.sBf * sTf);
+            const float sR = fmaf(de.sBf, cTf, de.cBf * sTf);
+            const Footprint fp = make_footprint(cR, sR);
+            w = footprint_weight(dist, qe * g.beamWidthF * de.invbq, fp);
+            if (FBP) w = w * g.dF * g.dF / qe / qe;
         } else {
-            const float hw = 0.5f * (fabsf(cTf) + fabsf(sTf));
-            const float uf = (float)u;
-            tlo = uf - hw;
-            thi = uf + hw;
+            w = footprint_weight((float)(u - de.t), g.beamWidthF, pfp);
         }
-        int dl = (int)roundf(fmaxf(tlo / dSf, (float)(-dmax - 1)));
-        int dr = (int)roundf(fminf(thi / dSf, (float)(dmax + 1)));
-        dl = max(dl, -dmax);
-        dr = min(dr, dmax);
-        Footprint pfp;
-        if (!FAN) {
-            pfp.h = bv.h; pfp.b1 = bv.b1; pfp.b2 = bv.b2; pfp.w = bv.w; pfp.iw2 = bv.iw2;
+        if (COUNT) {
+            if (w != 0.0f) nz += (nimg == 8 ? bv.cnt8 : bv.cnt4);
+            continue;
         }
-        for (int dt = dl; dt <= dr; ++dt) {
-            const DetEntry &de = p.det[dt + pC];
-            float w;
-            if (FAN) {
-                // distance from the detector's ray: cos B (u - t) + sin B v
-                const float dist = (float)fma(de.cB, u - de.t, de.sB * v);
-                const float cR = fmaf(de.cBf, cTf, -de.sBf * sTf);
-                const float sR = fmaf(de.sBf, cTf, de.cBf * sTf);
-                const Footprint fp = make_footprint(cR, sR);
-                w = footprint_weight(dist, qe * g.beamWidthF * de.invbq, fp);
-                if (FBP) w = w * g.dF * g.dF / qe / qe;
-            } else {
-                w = footprint_weight((float)(u - de.t), g.beamWidthF, pfp);
-            }
-            if (COUNT) {
-                if (w != 0.0f) nz += (nimg == 8 ? bv.cnt8 : bv.cnt4);
-                continue;
-            }
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int sg = j < 4 ? dt : -dt;
-                const int row = bv.row[j];
-                if (row >= 0) S[j] = fmaf(w, __ldg(sino + row + pC + sg), S[j]);
-                if (!FAN) {
-                    const int row2 = bv.row2[j];
-                    if (row2 >= 0) S[j] = fmaf(w, __ldg(sino + row2 + pC - sg), S[j]);
-                }
+        for (int j = 0; j < 8; ++j) {
+            const int sg = j < 4 ? dt : -dt;
+            const int row = bv.row[j];
+            if (row >= 0) S[j] = fmaf(w, __ldg(sino + row + pC + sg), S[j]);
+            if (!FAN) {
+                const int row2 = bv.row2[j];
+                if (row2 >= 0) S[j] = fmaf(w, __ldg(sino + row2 + pC - sg), S[j]);
             }
         }
     }
+}
 
-    if (COUNT) {
-        if (nz) atomicAdd(counter, nz);
-        return;
-    }
+__device__ __forceinline__ void decode_tile(int tile, int &tx, int &ty)
+{
+    tx = (int)((sqrtf(8.0f * (float)tile + 1.0f) - 1.0f) * 0.5f);
+    while ((tx + 1) * (tx + 2) / 2 <= tile) ++tx;
+    while (tx * (tx + 1) / 2 > tile) --tx;
+    ty = tile - tx * (tx + 1) / 2;
+}
+
+__device__ __forceinline__ void write_octant(const BwdParams &p, float *__restrict__ img, int x,
+                                             int y, int nimg, const float (&S)[8])
+{
+    const Geo &g = p.g;
     const int h2 = g.h2, N = g.n;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -423,8 +432,251 @@ k_backward(const BwdParams p, const float *__restrict__ sino, float *__restrict_
     }
 }
 
-int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp,
-                    unsigned long long *counter, cudaStream_t s, float scale)
+template <bool FAN, bool COUNT, bool FBP>
+__global__ void __launch_bounds__(kBwdTile * kBwdTile)
+k_backward(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img,
+           unsigned long long *__restrict__ counter)
+{
+    const Geo &g = p.g;
+    if (!COUNT && p.zero_axes && blockIdx.x == 0)
+        for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+            img[i] = 0.0f;
+            img[(size_t)i * g.n] = 0.0f;
+        }
+    int tx, ty;
+    decode_tile(blockIdx.x, tx, ty);
+    const int x = tx * kBwdTile + (int)(threadIdx.x % kBwdTile);
+    const int y = ty * kBwdTile + (int)(threadIdx.x / kBwdTile);
+    if (x > g.half || y > x) return;
+    const int nimg = (y == 0 || y == x) ? 4 : 8;
+    float S[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) S[j] = 0.0f;
+    unsigned long long nz = 0;
+    for (int i = 0; i < p.nv; ++i) bwd_view_direct<FAN, COUNT, FBP>(p, sino, i, x, y, nimg, S, nz);
+    if (COUNT) {
+        if (nz) atomicAdd(counter, nz);
+        return;
+    }
+    write_octant(p, img, x, y, nimg, S);
+}
+
+// ------------------------------------------------------ backward, staged tiles
+//
+// The same backprojection with the per-(view, detector) work hoisted out of the
+// per-pixel loop.  A block owns a 16 x 16 tile of octant pixels; for a batch of
+// VB base views it first stages, for every detector under the tile's shadow,
+// (a) the ray's footprint coefficients and its distance from the tile centre,
+// computed in FP64 and rounded, and (b) the eight mirrored sinogram samples the
+// weight will multiply.  Each pixel then needs only its offset from the tile
+// centre: dist = D_k + cos B_k du + sin B_k dv, a saturating-FMA footprint and
+// eight shared-memory reads per detector.  The staging capacity SEG (detectors
+// per view and tile) is chosen per plan from the exact maximum shadow width,
+// found once by k_tile_span_max; geometries whose shadows exceed 64 detectors
+// use the unstaged kernel.
+
+struct TileSpan {
+    int klo, nseg;
+};
+
+// Detectors any pixel of tile (tx, ty) can reach in base view bv, as the first
+// one (relative to the centre bin) and a count, with one spare on each side
+// (the pixels' own shadows are rounded to the nearest bin from FP32 corners).
+// nseg = 1 << 20 flags a tile the source sees from behind or edge-on.
+__device__ __forceinline__ TileSpan tile_span(const Geo &g, const BwdView &bv, int tx, int ty)
+{
+    const int dmax = (g.W - 1) / 2;
+    const float X0 = tx * kBwdTile - 0.5f, X1 = X0 + kBwdTile;
+    const float Y0 = ty * kBwdTile - 0.5f, Y1 = Y0 + kBwdTile;
+    const float cx[4] = {X0, X1, X1, X0}, cy[4] = {Y0, Y0, Y1, Y1};
+    float lo = 0.0f, hi = 0.0f;
+    bool bad = false;
+    for (int q = 0; q < 4; ++q) {
+        const float oc = fmaf(cx[q], bv.cf, cy[q] * bv.sf);
+        float tq = oc;
+        if (g.fan) {
+            const float qe = fmaf(cx[q], bv.sf, -cy[q] * bv.cf) + g.dF;
+            bad |= !(qe > 1e-3f * g.dF);
+            tq = g.dF * oc / qe;
+        }
+        lo = q == 0 ? tq : fminf(lo, tq);
+        hi = q == 0 ? tq : fmaxf(hi, tq);
+    }
+    TileSpan sp;
+    const float inv = (float)(1.0 / g.dSize), lim = (float)dmax + 2.0f;
+    const int klo = max(__float2int_rd(fminf(fmaxf(lo * inv, -lim), lim)) - 1, -dmax);
+    const int khi = min(__float2int_ru(fminf(fmaxf(hi * inv, -lim), lim)) + 1, dmax);
+    sp.klo = klo;
+    sp.nseg = bad ? (1 << 20) : khi - klo + 1;
+    return sp;
+}
+
+__global__ void k_tile_span_max(const BwdParams p, int tiles, int *__restrict__ out)
+{
+    int m = 0;
+    const long long total = (long long)tiles * p.nv;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int tx, ty;
+        decode_tile((int)(e / p.nv), tx, ty);
+        m = max(m, tile_span(p.g, p.view[e % p.nv], tx, ty).nseg);
+    }
+    atomicMax(out, m);
+}
+
+struct TileView {
+    double uc, vc;        // tile centre along / across the detector (FP64)
+    float cT, sT;
+    float ucf, qec;       // u of the centre; d - v of the centre
+    float hw;             // parallel: (|cos| + |sin|) / 2
+    int klo, nseg;
+};
+
+template <bool FAN, bool FBP, int SEG, int VB>
+__global__ void __launch_bounds__(kBwdTile * kBwdTile)
+k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
+{
+    const Geo &g = p.g;
+    __shared__ float4 ra[VB][SEG];                      // D, cos B, sin B, half beam / qe
+    __shared__ float4 rb[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: hw, tb, hwr, iw
+    __shared__ float4 rc[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: c1, c2, i2b
+    __shared__ float seg[VB][8][SEG];
+    __shared__ float seg2[FAN ? 1 : VB][8][SEG];
+    __shared__ TileView tv[VB];
+    __shared__ FootprintSat pfs[VB];
+    constexpr int kWarps = kBwdTile * kBwdTile / 32;
+
+    if (p.zero_axes && blockIdx.x == 0)
+        for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+            img[i] = 0.0f;
+            img[(size_t)i * g.n] = 0.0f;
+        }
+    int tx, ty;
+    decode_tile(blockIdx.x, tx, ty);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x = tx * kBwdTile + (int)(threadIdx.x % kBwdTile);
+    const int y = ty * kBwdTile + (int)(threadIdx.x / kBwdTile);
+    const bool valid = x <= g.half && y <= x;
+    const int nimg = (y == 0 || y == x) ? 4 : 8;
+    const double xc = tx * kBwdTile + 0.5 * (kBwdTile - 1), yc = ty * kBwdTile + 0.5 * (kBwdTile - 1);
+    const float dx = (float)(x - xc), dy = (float)(y - yc);
+    const int dmax = (g.W - 1) / 2, pC = g.pC;
+    const float invdS = (float)(1.0 / g.dSize), dF = g.dF;
+    const float hbpar = 0.5f * g.beamWidthF;
+    float S[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) S[j] = 0.0f;
+
+    for (int i0 = 0; i0 < p.nv; i0 += VB) {
+        const int nb = min(VB, p.nv - i0);
+        // A: per view, the tile's detector span and centre
+        if (threadIdx.x < nb) {
+            const int iv = threadIdx.x;
+            const BwdView &bv = p.view[i0 + iv];
+            const TileSpan sp = tile_span(g, bv, tx, ty);
+            TileView t;
+            t.cT = bv.cf;
+            t.sT = bv.sf;
+            t.uc = fma(xc, bv.c, yc * bv.s);
+            t.vc = fma(yc, bv.c, -xc * bv.s);
+            t.ucf = (float)t.uc;
+            t.qec = (float)(g.d - t.vc);
+            t.hw = 0.5f * (fabsf(bv.cf) + fabsf(bv.sf));
+            t.klo = sp.klo;
+            t.nseg = min(sp.nseg, SEG);   // the plan chose SEG above every span
+            tv[iv] = t;
+            if (!FAN) pfs[iv] = make_footprint_sat(bv.cf, bv.sf);
+        }
+        __syncthreads();
+        // B1: ray coefficients of the staged detectors, a warp per view
+        for (int iv = warp; iv < nb; iv += kWarps) {
+            const TileView &t = tv[iv];
+            for (int kk = lane; kk < t.nseg; kk += 32) {
+                const DetEntry &de = p.det[t.klo + kk + pC];
+                if (FAN) {
+                    const double D = fma(de.cB, t.uc - de.t, de.sB * t.vc);
+                    const float cR = fmaf(de.cBf, t.cT, -de.sBf * t.sT);
+                    const float sR = fmaf(de.sBf, t.cT, de.cBf * t.sT);
+                    const FootprintSat f = make_footprint_sat(cR, sR);
+                    ra[iv][kk] = make_float4((float)D, de.cBf, de.sBf, 0.5f * g.beamWidthF * de.invbq);
+                    rb[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.hw, f.tb, f.hwr, f.iw);
+                    rc[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.c1, f.c2, f.i2b, 0.0f);
+                } else {
+                    ra[iv][kk] = make_float4((float)(t.uc - de.t), 0.0f, 0.0f, 0.0f);
+                }
+            }
+        }
+        // B2: the mirrored sinogram samples, a warp per (view, image)
+        for (int pr = warp; pr < nb * 8; pr += kWarps) {
+            const int iv = pr >> 3, j = pr & 7;
+            const TileView &t = tv[iv];
+            const BwdView &bv = p.view[i0 + iv];
+            const int row = bv.row[j];
+            const int row2 = FAN ? -1 : bv.row2[j];
+            for (int kk = lane; kk < t.nseg; kk += 32) {
+                const int dt = t.klo + kk;
+                const int sg = j < 4 ? dt : -dt;
+                seg[iv][j][kk] = row >= 0 ? __ldg(sino + row + pC + sg) : 0.0f;
+                if (!FAN) seg2[FAN ? 0 : iv][j][kk] = row2 >= 0 ? __ldg(sino + row2 + pC - sg) : 0.0f;
+            }
+        }
+        __syncthreads();
+        // C: every pixel of the tile over the batch
+        if (valid) {
+            for (int iv = 0; iv < nb; ++iv) {
+                const TileView &t = tv[iv];
+                const float du = fmaf(dx, t.cT, dy * t.sT);
+                const float dv = fmaf(dy, t.cT, -dx * t.sT);
+                const float u = t.ucf + du;
+                float tlo, thi, qe = 0.0f;
+                if (FAN) {
+                    // the pixel's corner shadows (prj/cpuPrj.c:218-244); only
+                    // which detector each edge falls in matters here
+                    qe = t.qec - dv;
+                    const float hc = 0.5f * t.cT, hs = 0.5f * t.sT;
+                    const float A = hc + hs, B = hc - hs;
+                    const float t0 = __fdividef(dF * (u - A), qe + B);
+                    const float t1 = __fdividef(dF * (u + B), qe + A);
+                    const float t2 = __fdividef(dF * (u + A), qe - B);
+                    const float t3 = __fdividef(dF * (u - B), qe - A);
+                    tlo = fminf(fminf(t0, t1), fminf(t2, t3));
+                    thi = fmaxf(fmaxf(t0, t1), fmaxf(t2, t3));
+                } else {
+                    tlo = u - t.hw;
+                    thi = u + t.hw;
+                }
+                const float lim = (float)dmax + 1.0f;
+                int dl = __float2int_rn(fminf(fmaxf(tlo * invdS, -lim), lim));
+                int dr = __float2int_rn(fminf(fmaxf(thi * invdS, -lim), lim));
+                dl = max(max(dl, -dmax) - t.klo, 0);
+                dr = min(min(dr, dmax) - t.klo, t.nseg - 1);
+                const float fbpw = FBP ? __fdividef(dF, qe) * __fdividef(dF, qe) : 1.0f;
+                for (int kk = dl; kk <= dr; ++kk) {
+                    const float4 a = ra[iv][kk];
+                    float w;
+                    if (FAN) {
+                        const float dist = fmaf(a.y, du, fmaf(a.z, dv, a.x));
+                        const float4 b = rb[FAN ? iv : 0][FAN ? kk : 0], c = rc[FAN ? iv : 0][FAN ? kk : 0];
+                        const FootprintSat f = {b.x, b.y, b.z, b.w, c.x, c.y, c.z};
+                        w = footprint_weight_sat(dist, qe * a.w, f);
+                        if (FBP) w *= fbpw;
+                    } else {
+                        w = footprint_weight_sat(a.x + du, hbpar, pfs[iv]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        S[j] = fmaf(w, seg[iv][j][kk], S[j]);
+                        if (!FAN) S[j] = fmaf(w, seg2[FAN ? 0 : iv][j][kk], S[j]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (valid) write_octant(p, img, x, y, nimg, S);
+}
+
+static BwdParams bwd_params(const ctprj_plan *pl, int fbp, float scale)
 {
     BwdParams p;
     p.g = pl->g;
@@ -436,17 +688,62 @@ int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp
                   : scale;
     p.view = pl->d_bview;
     p.det = pl->d_det;
+    return p;
+}
+
+// widest tile shadow of the plan's geometry, in detectors (plan creation)
+int backward_max_span(const ctprj_plan *pl, int *max_span)
+{
+    const BwdParams p = bwd_params(pl, 0, 1.0f);
+    const int tiles = p.tiles_side * (p.tiles_side + 1) / 2;
+    int *d = nullptr;
+    int st = cuda_error(cudaMalloc((void **)&d, sizeof(int)), "span scratch");
+    if (st) return st;
+    int h = 0;
+    if (!(st = cuda_error(cudaMemset(d, 0, sizeof(int)), "span reset"))) {
+        k_tile_span_max<<<296, 256>>>(p, tiles, d);
+        if (!(st = cuda_error(cudaGetLastError(), "span launch")))
+            st = cuda_error(cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost), "span readback");
+    }
+    cudaFree(d);
+    *max_span = h;
+    return st;
+}
+
+int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp,
+                    unsigned long long *counter, cudaStream_t s, float scale)
+{
+    const BwdParams p = bwd_params(pl, fbp, scale);
+    const int T = p.tiles_side;
     dim3 grid(T * (T + 1) / 2), block(kBwdTile * kBwdTile);
     const bool fan = pl->g.fan != 0;
     if (counter) {
         if (fan) k_backward<true, true, false><<<grid, block, 0, s>>>(p, sino, img, counter);
         else k_backward<false, true, false><<<grid, block, 0, s>>>(p, sino, img, counter);
-    } else if (fbp) {
-        if (fan) k_backward<true, false, true><<<grid, block, 0, s>>>(p, sino, img, counter);
-        else k_backward<false, false, true><<<grid, block, 0, s>>>(p, sino, img, counter);
+    } else if (pl->bwd_seg == 0) {
+        if (fbp) {
+            if (fan) k_backward<true, false, true><<<grid, block, 0, s>>>(p, sino, img, counter);
+            else k_backward<false, false, true><<<grid, block, 0, s>>>(p, sino, img, counter);
+        } else {
+            if (fan) k_backward<true, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
+            else k_backward<false, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
+        }
+    } else if (pl->bwd_seg <= 32) {
+        if (fan) {
+            if (fbp) k_backward_tiled<true, true, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
+            else k_backward_tiled<true, false, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
+        } else {
+            if (fbp) k_backward_tiled<false, true, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
+            else k_backward_tiled<false, false, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
+        }
     } else {
-        if (fan) k_backward<true, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
-        else k_backward<false, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
+        if (fan) {
+            if (fbp) k_backward_tiled<true, true, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
+            else k_backward_tiled<true, false, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
+        } else {
+            if (fbp) k_backward_tiled<false, true, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
+            else k_backward_tiled<false, false, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
+        }
     }
     return cuda_error(cudaGetLastError(), "backward launch");
 }

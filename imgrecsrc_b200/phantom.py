@@ -53,3 +53,13 @@ def two_material_phantom(n, seed=0, count=10, fe_fraction=0.3):
         m = _ellipse_mask(X, Y, 0.6 * cx[i], 0.6 * cy[i], 0.5 * a[i], 0.5 * b[i], phi[i])
         img[m] = 7.8 if fe[i] else 2.7
     return img.astype(np.float32)
+
+
+def spectrum_bump(J, seed=0):
+    """Seeded smooth bump of J non-negative spectrum coefficients, positive
+    everywhere and normalised to sum 1."""
+    rng = np.random.default_rng(seed)
+    mu = rng.uniform(0.35, 0.65) * (J - 1)
+    sig = rng.uniform(0.08, 0.15) * J
+    I = np.exp(-0.5 * ((np.arange(J) - mu) / sig) ** 2) + 1e-3
+    return I / I.sum()

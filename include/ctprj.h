@@ -159,6 +159,11 @@ int ctprj_bhc_backward(ctprj_bhc *model, const float *d_x, const double *d_Ie,
 int ctprj_bhc_terms(ctprj_bhc *model, const float *d_sino, const double *d_Ie,
                     const float *d_imea, double *d_f, int save, void *stream);
 
+/* The rays x J basis matrix d_A[i*J + j] = b_j(Ts * d_sino[i]) in FP64
+ * (Spline.b1Iout with an empty spectrum, bhc/Spline.m:143), for spectrum
+ * solvers that work on the matrix. */
+int ctprj_bhc_basis(ctprj_bhc *model, const float *d_sino, double *d_A, void *stream);
+
 /* Device pointers of the saved per-ray state: s_i, 1 - m_i/BL_i and
  * (1 - m_i/BL_i) dBL/ds (np*prjWidth floats each). */
 int ctprj_bhc_state(ctprj_bhc *model, const float **d_s, const float **d_r, const float **d_w);

@@ -136,3 +136,26 @@ def test_central_finite_differences():
         errI.append(abs(fd - an) / (torch.linalg.norm(gI) * torch.linalg.norm(d)).item())
     assert max(errI) < 1e-5, max(errI)
     print("bhc finite differences: max rel err density %.2e, spectrum %.2e" % (max(errs), max(errI)))
+
+
+def test_basis_matrix_and_reference_call_structure():
+    """The materialised basis matrix (Spline.b1Iout with I empty) matches the
+    oracle, and the spectrum gradient formed the reference's way,
+    A^T (1 - m / (A Ie)) (bhc/poissLI.m:2-6), equals the fused one."""
+    g = GEOMS["fan"]
+    x, k, Ie, m, Ts = problem(g, J=30, seed=5)
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    dx = torch.from_numpy(x).cuda()
+    dI = torch.from_numpy(Ie).cuda()
+    dm = torch.from_numpy(m.astype(np.float32)).cuda()
+    sino = pr.forward(dx)
+    A = model.basis(sino)
+    s = Ts * sino.double().cpu().numpy().ravel()
+    Bo, _, _ = BO.b1_basis(k, s)
+    assert rel(A.cpu().numpy(), Bo) < 1e-12
+    Ir = A @ dI
+    gI_ref = A.t() @ (1 - dm.double().ravel() / Ir)
+    model.forward(dx, dI, dm)
+    _, gI = model.backward(grad_x=False)
+    assert rel(gI.cpu().numpy(), gI_ref.cpu().numpy()) < 1e-6
