@@ -252,6 +252,7 @@ def our_arm(args):
     traffic = PROFILED_TRAFFIC.get("k_backward" if bwd_ms >= fwd_ms else "k_forward")
 
     bhc_line = bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
+    batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
 
     # end to end through the reference-facing C ABI: setup() once, then per
     # step gpuPrj(FWD) and gpuPrj(BWD) on pinned host buffers (every call
@@ -300,6 +301,7 @@ def our_arm(args):
         "gpu_launches": 3 * args.steps,
         "clocks": clk,
         "bhc": bhc_line,
+        "batch": batch_line,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         v, t, info = cpu_reference_run(1, 0)
@@ -377,6 +379,67 @@ def bhc_leg(ct, g, pr, flush, stream, steps):
     out["speedup_vs_plain_min"] = out["plain_min_ms"] / out["fused_ms"]
     out["fused_launches_per_iter"] = 6
     model.close()
+    return out
+
+
+def batch_leg(ct, flush, stream, steps):
+    """64 slices of mixed geometry (n in {128..1024}, 90..720 views, half
+    parallel, half fan): forward + backprojection of every slice, as one tuned,
+    graph-captured persistent launch per direction, against a loop of per-slice
+    ctprj_forward / ctprj_backward calls on the same stream."""
+    import numpy as np
+    import torch
+
+    from imgrecsrc_b200 import batch, phantom
+    geoms = batch.cfg4_geometries(64, seed=0)
+    rng = np.random.default_rng(3)
+    imgs = [torch.from_numpy(phantom.ellipse_phantom(g.n, seed=i)).cuda() for i, g in enumerate(geoms)]
+    sinos = [torch.empty(g.np, g.prjWidth, device="cuda") for g in geoms]
+    bimgs = [torch.empty(g.n, g.n, device="cuda") for g in geoms]
+    projs = [ct.Projector(g) for g in geoms]
+    updates = 0
+    for p in projs:
+        f, bw = p.count_updates()
+        updates += f + bw
+    b = batch.Batch(geoms)
+    b.bind(imgs, sinos, sinos, bimgs)
+    cfg = b.autotune(None)
+    b.capture()
+
+    def batched():
+        b.forward()
+        b.backward()
+
+    def looped():
+        for p, x, y, z in zip(projs, imgs, sinos, bimgs):
+            p.forward(x, out=y)
+            p.backward(y, out=z)
+
+    out = {"workload": "64 seeded slices: n in {128,256,384,512,768,1024}, views in {90,180,360,720} "
+                       "(fan 90 -> 92), half parallel [0,pi) / half fan [0,2pi) d=4n, prjWidth=ceil(1.42n)",
+           "updates_per_step": updates, "tuned": cfg}
+    for name, fn in (("batched", batched), ("per_slice", looped)):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ms = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        ms /= steps
+        out[name + "_ms"] = ms
+        out[name + "_gray_px_per_s"] = updates / (ms * 1e-3) / 1e9
+    out["speedup"] = out["per_slice_ms"] / out["batched_ms"]
+    out["batched_launches_per_step"] = 5   # 2 counter resets, transpose, forward, backward
+    b.close()
+    for p in projs:
+        p.close()
     return out
 
 

@@ -82,6 +82,14 @@ def lib():
         "parPrjConf": ([VP, VP, VP, ctypes.POINTER(ParConf), ctypes.c_size_t], ctypes.c_int),
         "parPrjThread": ([], ctypes.c_int),
         "parPrjRun": ([], ctypes.c_int),
+        "ctprj_batch_create": ([GP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(VP)], ctypes.c_int),
+        "ctprj_batch_destroy": ([VP], None),
+        "ctprj_batch_bind": ([VP, VP, VP, VP, VP], ctypes.c_int),
+        "ctprj_batch_forward": ([VP, VP], ctypes.c_int),
+        "ctprj_batch_backward": ([VP, VP], ctypes.c_int),
+        "ctprj_batch_capture": ([VP, VP], ctypes.c_int),
+        "ctprj_batch_autotune": ([VP, VP, ctypes.c_char_p], ctypes.c_int),
+        "ctprj_batch_config": ([VP, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

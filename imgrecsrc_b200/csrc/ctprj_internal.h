@@ -85,6 +85,31 @@ struct BwdParams {
     const DetEntry *det;
 };
 
+// One slice of a batch (batch.cu): its plan's parameter blocks and buffers.
+struct BatchSlice {
+    FwdParams fp;
+    BwdParams bp;
+    const float *img;       // forward input
+    float *imgT;            // forward scratch (the slice plan's)
+    float *sino;            // forward output
+    const float *bsino;     // backward input
+    float *bimg;            // backward output
+    int tiled;              // backward: 1 staged tiles, 0 unstaged
+};
+
+// Work lists of a batched launch: items of the slices in `order`, item e
+// belonging to the slice at position i when prefix[i] <= e < prefix[i + 1].
+struct BatchArgs {
+    const BatchSlice *slices;
+    int nslices;
+    const int *order;
+    const long long *prefix;       // forward blocks or backward tiles
+    long long total;
+    const long long *tprefix;      // transpose tiles (natural order)
+    long long ttotal;
+    unsigned long long *counter;   // work counter, zero before each launch
+};
+
 }  // namespace ctprj
 
 struct ctprj_plan {
@@ -119,6 +144,13 @@ int launch_forward_bhc(const ctprj_plan *p, const float *img, const float *imgT,
                        const BhcArgs &a, int *nparts, cudaStream_t s);
 int forward_blocks(const ctprj_plan *p);
 int backward_max_span(const ctprj_plan *p, int *max_span);
+FwdParams make_fwd_params(const ctprj_plan *p);
+BwdParams make_bwd_params(const ctprj_plan *p);
+// persistent batch launches (projector.cu)
+int launch_transpose_batch(const BatchArgs &a, cudaStream_t s);
+int launch_forward_batch(const BatchArgs &a, int views, int ctas, cudaStream_t s);
+int launch_backward_batch(const BatchArgs &a, int seg, int vb, int ctas, cudaStream_t s);
+int batch_max_ctas(int kind, int param, int *per_sm);
 int launch_backward(const ctprj_plan *p, const float *sino, float *img, int fbp,
                     unsigned long long *counter, cudaStream_t s, float scale = 1.0f);
 

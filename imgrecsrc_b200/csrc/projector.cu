@@ -95,26 +95,23 @@ __device__ __forceinline__ double block_sum(double v, double *red)
     return t;
 }
 
-template <bool FAN, int MODE>
-__global__ void __launch_bounds__(kFwdThreads)
-k_forward(const FwdParams p, const float *__restrict__ img, const float *__restrict__ imgT,
-          float *__restrict__ sino, unsigned long long *__restrict__ counter)
+// The rays of one forward block: V adjacent base views (one per warp) x 32
+// adjacent detectors; block (bx, by) of the per-plan grid.  Returns this
+// thread's Poisson terms in polychromatic mode.
+template <bool FAN, int MODE, int V>
+__device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int by,
+                                               const float *__restrict__ img,
+                                               const float *__restrict__ imgT,
+                                               float *__restrict__ sino,
+                                               unsigned long long *__restrict__ counter,
+                                               const double *tab, const double *Ie)
 {
     const Geo &g = p.g;
-    const int b = blockIdx.x * kFwdViews + (int)(threadIdx.x >> 5);
-    const int r = blockIdx.y * 32 + (int)(threadIdx.x & 31);
+    const int b = bx * V + (int)(threadIdx.x >> 5);
+    const int r = by * 32 + (int)(threadIdx.x & 31);
     double fsum = 0.0;            // polychromatic mode: this thread's Poisson terms
-    const double *tab = nullptr, *Ie = nullptr;
-    if constexpr (MODE == kModeBhc) {
-        __shared__ double sm[kMaxJ * (kSplStride + 1)];
-        for (int i = threadIdx.x; i < p.bhc.J * kSplStride; i += blockDim.x) sm[i] = p.bhc.tab[i];
-        for (int i = threadIdx.x; i < p.bhc.J; i += blockDim.x) sm[kMaxJ * kSplStride + i] = p.bhc.Ie[i];
-        __syncthreads();
-        tab = sm;
-        Ie = sm + kMaxJ * kSplStride;
-    }
     // detector 0 of an even-width sinogram: no ray, zero projection
-    if (MODE != kModeCount && p.zero_col0 && blockIdx.x == 0 && blockIdx.y == 0)
+    if (MODE != kModeCount && p.zero_col0 && bx == 0 && by == 0)
         for (int v = threadIdx.x; v < g.np; v += blockDim.x) {
             if constexpr (MODE == kModeBhc) fsum += bhc_entry(p.bhc, tab, Ie, 0.0f, (size_t)v * g.W);
             else sino[(size_t)v * g.W] = 0.0f;
@@ -251,7 +248,25 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
         }
         if (MODE == kModeCount && nz * entries) atomicAdd(counter, nz * entries);
     }
+    return fsum;
+}
 
+template <bool FAN, int MODE>
+__global__ void __launch_bounds__(kFwdThreads)
+k_forward(const FwdParams p, const float *__restrict__ img, const float *__restrict__ imgT,
+          float *__restrict__ sino, unsigned long long *__restrict__ counter)
+{
+    const double *tab = nullptr, *Ie = nullptr;
+    if constexpr (MODE == kModeBhc) {
+        __shared__ double sm[kMaxJ * (kSplStride + 1)];
+        for (int i = threadIdx.x; i < p.bhc.J * kSplStride; i += blockDim.x) sm[i] = p.bhc.tab[i];
+        for (int i = threadIdx.x; i < p.bhc.J; i += blockDim.x) sm[kMaxJ * kSplStride + i] = p.bhc.Ie[i];
+        __syncthreads();
+        tab = sm;
+        Ie = sm + kMaxJ * kSplStride;
+    }
+    const double fsum = forward_rays<FAN, MODE, kFwdViews>(p, blockIdx.x, blockIdx.y, img, imgT,
+                                                           sino, counter, tab, Ie);
     if constexpr (MODE == kModeBhc) {
         __shared__ double red[kFwdThreads / 32];
         const double t = block_sum(fsum, red);
@@ -432,6 +447,32 @@ __device__ __forceinline__ void write_octant(const BwdParams &p, float *__restri
     }
 }
 
+// one tile of the unstaged backprojection (plain mode), for persistent use
+template <bool FAN>
+__device__ __forceinline__ void backward_tile_direct(const BwdParams &p, int tile,
+                                                     const float *__restrict__ sino,
+                                                     float *__restrict__ img)
+{
+    const Geo &g = p.g;
+    if (p.zero_axes && tile == 0)
+        for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+            img[i] = 0.0f;
+            img[(size_t)i * g.n] = 0.0f;
+        }
+    int tx, ty;
+    decode_tile(tile, tx, ty);
+    const int x = tx * kBwdTile + (int)(threadIdx.x % kBwdTile);
+    const int y = ty * kBwdTile + (int)(threadIdx.x / kBwdTile);
+    if (x > g.half || y > x) return;
+    const int nimg = (y == 0 || y == x) ? 4 : 8;
+    float S[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) S[j] = 0.0f;
+    unsigned long long nz = 0;
+    for (int i = 0; i < p.nv; ++i) bwd_view_direct<FAN, false, false>(p, sino, i, x, y, nimg, S, nz);
+    write_octant(p, img, x, y, nimg, S);
+}
+
 template <bool FAN, bool COUNT, bool FBP>
 __global__ void __launch_bounds__(kBwdTile * kBwdTile)
 k_backward(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img,
@@ -532,27 +573,42 @@ struct TileView {
     int klo, nseg;
 };
 
+// shared memory of one staged tile
+template <bool FAN, int SEG, int VB>
+struct TiledSmem {
+    float4 ra[VB][SEG];                      // D, cos B, sin B, half beam / qe
+    float4 rb[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: hw, tb, hwr, iw
+    float4 rc[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: c1, c2, i2b
+    float seg[VB][8][SEG];
+    float seg2[FAN ? 1 : VB][8][SEG];
+    TileView tv[VB];
+    FootprintSat pfs[VB];
+};
+
+// One tile of the staged backprojection (all threads of the block take part).
 template <bool FAN, bool FBP, int SEG, int VB>
-__global__ void __launch_bounds__(kBwdTile * kBwdTile)
-k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
+__device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
+                                              const float *__restrict__ sino,
+                                              float *__restrict__ img,
+                                              TiledSmem<FAN, SEG, VB> &sm)
 {
     const Geo &g = p.g;
-    __shared__ float4 ra[VB][SEG];                      // D, cos B, sin B, half beam / qe
-    __shared__ float4 rb[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: hw, tb, hwr, iw
-    __shared__ float4 rc[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: c1, c2, i2b
-    __shared__ float seg[VB][8][SEG];
-    __shared__ float seg2[FAN ? 1 : VB][8][SEG];
-    __shared__ TileView tv[VB];
-    __shared__ FootprintSat pfs[VB];
+    auto &ra = sm.ra;
+    auto &rb = sm.rb;
+    auto &rc = sm.rc;
+    auto &seg = sm.seg;
+    auto &seg2 = sm.seg2;
+    auto &tv = sm.tv;
+    auto &pfs = sm.pfs;
     constexpr int kWarps = kBwdTile * kBwdTile / 32;
 
-    if (p.zero_axes && blockIdx.x == 0)
+    if (p.zero_axes && tile == 0)
         for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
             img[i] = 0.0f;
             img[(size_t)i * g.n] = 0.0f;
         }
     int tx, ty;
-    decode_tile(blockIdx.x, tx, ty);
+    decode_tile(tile, tx, ty);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int x = tx * kBwdTile + (int)(threadIdx.x % kBwdTile);
     const int y = ty * kBwdTile + (int)(threadIdx.x / kBwdTile);
@@ -676,6 +732,14 @@ k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__res
     if (valid) write_octant(p, img, x, y, nimg, S);
 }
 
+template <bool FAN, bool FBP, int SEG, int VB>
+__global__ void __launch_bounds__(kBwdTile * kBwdTile)
+k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
+{
+    __shared__ TiledSmem<FAN, SEG, VB> sm;
+    backward_tile<FAN, FBP, SEG, VB>(p, blockIdx.x, sino, img, sm);
+}
+
 static BwdParams bwd_params(const ctprj_plan *pl, int fbp, float scale)
 {
     BwdParams p;
@@ -747,5 +811,155 @@ int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp
     }
     return cuda_error(cudaGetLastError(), "backward launch");
 }
+
+// ------------------------------------------------------------ batched launches
+//
+// One persistent launch serves a batch of slices of different geometries: each
+// block repeatedly takes the next work item from a device counter -- a forward
+// block (V views x 32 rays) or a backprojection tile of some slice -- finds its
+// slice by binary search over the item prefix sums, and runs the same block
+// body as the per-slice kernels.  Work is handed out in the slice order the
+// host chose (e.g. largest slices first), so the tail of the launch is short.
+
+__device__ __forceinline__ int find_slot(const long long *prefix, int n, long long item)
+{
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (prefix[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ long long next_item(unsigned long long *counter, long long *slot)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) *slot = (long long)atomicAdd(counter, 1ULL);
+    __syncthreads();
+    return *slot;
+}
+
+__global__ void __launch_bounds__(256) k_transpose_batch(const BatchArgs a)
+{
+    __shared__ float tile[32][33];
+    for (long long e = blockIdx.x; e < a.ttotal; e += gridDim.x) {
+        const int i = find_slot(a.tprefix, a.nslices, e);
+        const BatchSlice &sl = a.slices[i];
+        const int n = sl.fp.g.n, tn = (n + 31) / 32;
+        const int local = (int)(e - a.tprefix[i]);
+        const int bx = (local % tn) * 32, by = (local / tn) * 32;
+        __syncthreads();
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int row = by + r, col = bx + threadIdx.x;
+            if (row < n && col < n) tile[r][threadIdx.x] = sl.img[(size_t)row * n + col];
+        }
+        __syncthreads();
+        for (int r = threadIdx.y; r < 32; r += 8) {
+            const int row = bx + r, col = by + threadIdx.x;
+            if (row < n && col < n) sl.imgT[(size_t)row * n + col] = tile[threadIdx.x][r];
+        }
+    }
+}
+
+template <int V>
+__global__ void __launch_bounds__(32 * V, 24 / V) k_forward_batch(const BatchArgs a)
+{
+    __shared__ long long slot;
+    for (;;) {
+        const long long item = next_item(a.counter, &slot);
+        if (item >= a.total) return;
+        const int i = find_slot(a.prefix, a.nslices, item);
+        const BatchSlice &sl = a.slices[a.order[i]];
+        const int local = (int)(item - a.prefix[i]);
+        const int gx = (sl.fp.nb + V - 1) / V;
+        const int bx = local % gx, by = local / gx;
+        if (sl.fp.g.fan)
+            forward_rays<true, kModePlain, V>(sl.fp, bx, by, sl.img, sl.imgT, sl.sino, nullptr,
+                                              nullptr, nullptr);
+        else
+            forward_rays<false, kModePlain, V>(sl.fp, bx, by, sl.img, sl.imgT, sl.sino, nullptr,
+                                               nullptr, nullptr);
+    }
+}
+
+template <int SEG, int VB>
+constexpr size_t tiled_smem_bytes()
+{
+    return sizeof(TiledSmem<true, SEG, VB>) > sizeof(TiledSmem<false, SEG, VB>)
+               ? sizeof(TiledSmem<true, SEG, VB>)
+               : sizeof(TiledSmem<false, SEG, VB>);
+}
+
+template <int SEG, int VB>
+__global__ void __launch_bounds__(kBwdTile * kBwdTile, 4) k_backward_batch(const BatchArgs a)
+{
+    __shared__ __align__(16) unsigned char raw[tiled_smem_bytes<SEG, VB>()];
+    __shared__ long long slot;
+    for (;;) {
+        const long long item = next_item(a.counter, &slot);
+        if (item >= a.total) return;
+        const int i = find_slot(a.prefix, a.nslices, item);
+        const BatchSlice &sl = a.slices[a.order[i]];
+        const int tile = (int)(item - a.prefix[i]);
+        const bool fan = sl.bp.g.fan != 0;
+        if (sl.tiled) {
+            if (fan)
+                backward_tile<true, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
+                                                    *reinterpret_cast<TiledSmem<true, SEG, VB> *>(raw));
+            else
+                backward_tile<false, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
+                                                     *reinterpret_cast<TiledSmem<false, SEG, VB> *>(raw));
+        } else {
+            if (fan) backward_tile_direct<true>(sl.bp, tile, sl.bsino, sl.bimg);
+            else backward_tile_direct<false>(sl.bp, tile, sl.bsino, sl.bimg);
+        }
+    }
+}
+
+int launch_transpose_batch(const BatchArgs &a, cudaStream_t s)
+{
+    const long long blocks = a.ttotal < 65536 ? a.ttotal : 65536;
+    k_transpose_batch<<<(int)(blocks > 0 ? blocks : 1), dim3(32, 8), 0, s>>>(a);
+    return cuda_error(cudaGetLastError(), "batched transpose launch");
+}
+
+int launch_forward_batch(const BatchArgs &a, int views, int ctas, cudaStream_t s)
+{
+    switch (views) {
+    case 2: k_forward_batch<2><<<ctas, 64, 0, s>>>(a); break;
+    case 8: k_forward_batch<8><<<ctas, 256, 0, s>>>(a); break;
+    default: k_forward_batch<4><<<ctas, 128, 0, s>>>(a); break;
+    }
+    return cuda_error(cudaGetLastError(), "batched forward launch");
+}
+
+int launch_backward_batch(const BatchArgs &a, int seg, int vb, int ctas, cudaStream_t s)
+{
+    if (seg <= 32 && vb == 16) k_backward_batch<32, 16><<<ctas, 256, 0, s>>>(a);
+    else if (seg <= 32) k_backward_batch<32, 8><<<ctas, 256, 0, s>>>(a);
+    else k_backward_batch<64, 8><<<ctas, 256, 0, s>>>(a);
+    return cuda_error(cudaGetLastError(), "batched backward launch");
+}
+
+// resident blocks per SM of a batched kernel: kind 0 forward (param = views),
+// kind 1 backward (param = seg * 100 + vb)
+int batch_max_ctas(int kind, int param, int *per_sm)
+{
+    cudaError_t e;
+    if (kind == 0) {
+        if (param == 2) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_forward_batch<2>, 64, 0);
+        else if (param == 8) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_forward_batch<8>, 256, 0);
+        else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_forward_batch<4>, 128, 0);
+    } else {
+        if (param == 3216) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_backward_batch<32, 16>, 256, 0);
+        else if (param == 3208) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_backward_batch<32, 8>, 256, 0);
+        else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_backward_batch<64, 8>, 256, 0);
+    }
+    return cuda_error(e, "occupancy query");
+}
+
+FwdParams make_fwd_params(const ctprj_plan *pl) { return fwd_params(pl); }
+BwdParams make_bwd_params(const ctprj_plan *pl) { return bwd_params(pl, 0, 1.0f); }
 
 }  // namespace ctprj
