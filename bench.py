@@ -253,6 +253,7 @@ def our_arm(args):
 
     bhc_line = bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
     batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
+    loop_line = loop_leg(ct, g, pr, args.loop_iters) if args.loop_iters > 0 else None
 
     # end to end through the reference-facing C ABI: setup() once, then per
     # step gpuPrj(FWD) and gpuPrj(BWD) on pinned host buffers (every call
@@ -302,6 +303,7 @@ def our_arm(args):
         "clocks": clk,
         "bhc": bhc_line,
         "batch": batch_line,
+        "bhc_loop": loop_line,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         v, t, info = cpu_reference_run(1, 0)
@@ -382,6 +384,53 @@ def bhc_leg(ct, g, pr, flush, stream, steps):
     return out
 
 
+def loop_leg(ct, g, pr, iters):
+    """The alternating BHC reconstruction at 2048^2 (J = 30, Poisson counts at
+    I0 = 1e5): `iters` iterations of a density step (NPG: extrapolation,
+    fused likelihood + adjoint, majorisation line search) and an FP64 spectrum
+    step (Newton with an active-set QP on Ie >= 0), on the fused path and on
+    the plain FP32 unfused path; iterations per second of each, likelihood
+    evaluations and spectrum time, and how far apart their results are."""
+    import numpy as np
+    import torch
+
+    from imgrecsrc_b200 import bhc, phantom
+    J, I0 = BHC["J"], BHC["I0"]
+    Ts = BHC["fov_cm"] / g.n
+    x_true = torch.from_numpy(phantom.two_material_phantom(g.n, seed=2)).cuda()
+    nodes = bhc.kappa_nodes(J)
+    I_true = torch.from_numpy(phantom.spectrum_bump(J, seed=2)).cuda()
+    model = bhc.BHCModel(pr, nodes, Ts)
+    A = model.basis(pr.forward(x_true))
+    BL = (A @ I_true).reshape(g.np, g.prjWidth)
+    gen = torch.Generator(device="cuda").manual_seed(7)
+    imea = (torch.poisson(I0 * BL, generator=gen) / I0).float().contiguous()
+    del A, BL
+    out = {"workload": "fan 2048^2, 1440 views, 2048 bins, d=8192; J=30; I0=1e5; start x=1 g/cm^3, "
+                       "Ie uniform; %d iterations of density (NPG) + spectrum (<= 2 Newton steps)" % iters}
+    res = {}
+    for name, unfused in (("fused", False), ("unfused", True)):
+        x = torch.full((g.n, g.n), 1.0, device="cuda")
+        Ie = torch.full((J,), 1.0 / J, dtype=torch.float64, device="cuda")
+        st = model.reconstruct(x, Ie, imea, iterations=iters, x_step=1e-3, unfused=unfused)
+        res[name] = (x, Ie)
+        out[name + "_iter_per_s"] = st["iterations"] / (st["ms"] * 1e-3)
+        out[name + "_ms"] = st["ms"]
+        out[name + "_final_cost"] = st["final_cost"]
+        out[name + "_first_cost"] = st["cost"][0] if st["cost"] else None
+        out[name + "_evaluations"] = st["evaluations"]
+        out[name + "_ms_spectrum"] = st["ms_spectrum"]
+        out[name + "_restarts"] = st["restarts"]
+        out[name + "_newton_steps"] = st["newton_steps"]
+    out["speedup_vs_unfused"] = out["fused_iter_per_s"] / out["unfused_iter_per_s"]
+    (xf, If), (xu, Iu) = res["fused"], res["unfused"]
+    out["fused_vs_unfused_rel_x"] = (torch.linalg.norm((xf - xu).double()) / torch.linalg.norm(xu.double())).item()
+    out["fused_vs_unfused_rel_Ie"] = (torch.linalg.norm(If - Iu) / torch.linalg.norm(Iu)).item()
+    out["rel_err_vs_truth_x"] = (torch.linalg.norm((xf - x_true).double()) / torch.linalg.norm(x_true.double())).item()
+    model.close()
+    return out
+
+
 def batch_leg(ct, flush, stream, steps):
     """64 slices of mixed geometry (n in {128..1024}, 90..720 views, half
     parallel, half fan): forward + backprojection of every slice, as one tuned,
@@ -455,6 +504,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--loop-iters", type=int, default=50,
+                    help="alternating BHC iterations of the reconstruction leg (0: skip)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

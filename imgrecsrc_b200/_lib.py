@@ -25,6 +25,25 @@ class ParConf(ctypes.Structure):
                 ("theta", ctypes.POINTER(ctypes.c_double)), ("fwd", ctypes.c_int)]
 
 
+MAX_TRACE = 256
+
+
+class LoopOpts(ctypes.Structure):
+    """ctprj_bhc_loop_opts of include/ctprj_bhc_loop.h."""
+    _fields_ = [("iterations", ctypes.c_int), ("x_step", ctypes.c_double),
+                ("spectrum_newton_steps", ctypes.c_int), ("skip_spectrum", ctypes.c_int),
+                ("unfused", ctypes.c_int)]
+
+
+class LoopStats(ctypes.Structure):
+    """ctprj_bhc_loop_stats of include/ctprj_bhc_loop.h."""
+    _fields_ = [("iterations", ctypes.c_int), ("final_cost", ctypes.c_double),
+                ("final_x_step", ctypes.c_double), ("cost", ctypes.c_double * MAX_TRACE),
+                ("x_step", ctypes.c_double * MAX_TRACE), ("ms", ctypes.c_float),
+                ("ms_spectrum", ctypes.c_float), ("evaluations", ctypes.c_int),
+                ("restarts", ctypes.c_int), ("newton_steps", ctypes.c_int)]
+
+
 class Geometry(ctypes.Structure):
     """struct ctprj_geometry -- the reference's projector configuration
     (prj/prj.h:42-57): n, prjWidth, np, prjFull, dSize, effectiveRate, d."""
@@ -57,9 +76,10 @@ def lib():
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB):
+    path = os.environ.get("CTPRJ_LIB") or LIB    # another build of the same library
+    if not os.path.exists(path):
         raise RuntimeError("libctprj.so is missing: build it with `python -m imgrecsrc_b200.build`")
-    L = ctypes.CDLL(LIB)
+    L = ctypes.CDLL(path)
     GP = ctypes.POINTER(Geometry)
     sig = {
         "setup": ([ctypes.c_int] * 4 + [ctypes.c_float] * 3, None),
@@ -90,6 +110,11 @@ def lib():
         "ctprj_batch_capture": ([VP, VP], ctypes.c_int),
         "ctprj_batch_autotune": ([VP, VP, ctypes.c_char_p], ctypes.c_int),
         "ctprj_batch_config": ([VP, ctypes.c_char_p, ctypes.c_int], ctypes.c_int),
+        "ctprj_bhc_spectrum_step": ([VP, VP, VP, ctypes.c_int, ctypes.POINTER(ctypes.c_double), VP], ctypes.c_int),
+        "ctprj_bhc_reconstruct": ([VP, VP, VP, VP, ctypes.POINTER(LoopOpts), ctypes.POINTER(LoopStats), VP], ctypes.c_int),
+        "ctprj_stream_flags_create": ([ctypes.c_int, ctypes.POINTER(VP), ctypes.POINTER(VP)], ctypes.c_int),
+        "ctprj_stream_flags_destroy": ([VP], None),
+        "ctprj_batch_stream_backward": ([VP, VP, ctypes.c_double, VP, VP], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

@@ -5,7 +5,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import Geometry, check, lib
+from ._lib import CTPRJ_OK, CTPRJ_ETIMEOUT, Geometry, check, lib
 from .projector import _stream_handle
 
 
@@ -89,3 +89,40 @@ class Batch:
         buf = ctypes.create_string_buffer(256)
         check(lib().ctprj_batch_config(self._b, buf, 256))
         return buf.value.decode()
+
+
+class StreamFlags:
+    """Host-mapped publication flags for ctprj_batch_stream_backward: set
+    flag i once slice i's sinogram is on the device."""
+
+    def __init__(self, n):
+        self._h = ctypes.c_void_p()
+        self._d = ctypes.c_void_p()
+        check(lib().ctprj_stream_flags_create(int(n), ctypes.byref(self._h), ctypes.byref(self._d)))
+        self.n = int(n)
+        self.flags = np.ctypeslib.as_array(ctypes.cast(self._h, ctypes.POINTER(ctypes.c_int)), shape=(self.n,))
+
+    def publish(self, i):
+        self.flags[i] = 1
+
+    def close(self):
+        if self._h:
+            lib().ctprj_stream_flags_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def stream_backward(b, flags, timeout_s, stream=None):
+    """Streaming backprojection of a bound Batch; returns (status code,
+    per-slice timed-out flags).  CTPRJ_ETIMEOUT is returned, not raised."""
+    st = (ctypes.c_int * len(b.geometries))()
+    code = lib().ctprj_batch_stream_backward(b._b, flags._d, float(timeout_s), st,
+                                             _stream_handle(stream, b.device))
+    if code not in (CTPRJ_OK, CTPRJ_ETIMEOUT):
+        check(code)
+    return code, list(st)

@@ -12,7 +12,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import check, lib
+from ._lib import LoopOpts, LoopStats, check, lib
 from .projector import _dev_ptr, _stream_handle
 
 
@@ -111,3 +111,35 @@ class BHCModel:
                                        _dptr(gI, self.J, torch.float64) if gI is not None else None,
                                        _stream_handle(stream, pr.device)))
         return gx, gI
+
+    def spectrum_step(self, imea, Ie, newton_steps=2, stream=None):
+        """FP64 Newton update of Ie >= 0 (in place, at most newton_steps steps)
+        on the projections of the last saved forward; returns the likelihood
+        at the returned Ie."""
+        import torch
+        f = ctypes.c_double()
+        check(lib().ctprj_bhc_spectrum_step(self._m, _dptr(imea, self.nrays, torch.float32),
+                                            _dptr(Ie, self.J, torch.float64), int(newton_steps),
+                                            ctypes.byref(f), _stream_handle(stream, self.projector.device)))
+        return f.value
+
+    def reconstruct(self, x, Ie, imea, iterations, x_step=1.0, spectrum_newton_steps=2,
+                    skip_spectrum=False, unfused=False, stream=None):
+        """The alternating density / spectrum loop, x and Ie updated in place.
+        Returns a dict with the cost after each iteration, the accepted density
+        steps and the device time."""
+        import torch
+        pr = self.projector
+        opts = LoopOpts(int(iterations), float(x_step), int(spectrum_newton_steps),
+                        1 if skip_spectrum else 0, 1 if unfused else 0)
+        st = LoopStats()
+        check(lib().ctprj_bhc_reconstruct(self._m, _dev_ptr(x, pr.img_shape, pr.device),
+                                          _dptr(Ie, self.J, torch.float64),
+                                          _dptr(imea, self.nrays, torch.float32), ctypes.byref(opts),
+                                          ctypes.byref(st), _stream_handle(stream, pr.device)))
+        n = min(st.iterations, len(st.cost))
+        return {"iterations": st.iterations, "final_cost": st.final_cost, "ms": st.ms,
+                "cost": list(st.cost[:n]), "x_step": list(st.x_step[:n]),
+                "final_x_step": st.final_x_step, "ms_spectrum": st.ms_spectrum,
+                "evaluations": st.evaluations, "restarts": st.restarts,
+                "newton_steps": st.newton_steps}

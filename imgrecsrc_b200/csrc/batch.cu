@@ -43,6 +43,7 @@ struct ctprj_batch {
     int *d_order_f = nullptr, *d_order_b = nullptr;
     long long *d_fprefix = nullptr, *d_bprefix = nullptr, *d_tprefix = nullptr;
     unsigned long long *d_counter = nullptr;   // [0] forward, [1] backward
+    int *d_status = nullptr;                   // streaming: per slice, 1 = timed out
     long long ftotal = 0, btotal = 0, ttotal = 0;
     int seg = 0;                  // staging capacity used by the batched backprojection
     int bound = 0;                // buffers bound
@@ -231,7 +232,8 @@ extern "C" int ctprj_batch_create(const ctprj_geometry *geoms, int nslices, int 
             !(st = cuda_error(cudaMalloc((void **)&b->d_fprefix, sizeof(long long) * (n + 1)), "batch tables")) &&
             !(st = cuda_error(cudaMalloc((void **)&b->d_bprefix, sizeof(long long) * (n + 1)), "batch tables")) &&
             !(st = cuda_error(cudaMalloc((void **)&b->d_tprefix, sizeof(long long) * (n + 1)), "batch tables")) &&
-            !(st = cuda_error(cudaMalloc((void **)&b->d_counter, 2 * sizeof(unsigned long long)), "batch tables")))
+            !(st = cuda_error(cudaMalloc((void **)&b->d_counter, 2 * sizeof(unsigned long long)), "batch tables")) &&
+            !(st = cuda_error(cudaMalloc((void **)&b->d_status, sizeof(int) * n), "batch tables")))
             st = upload_lists(b);
     }
     if (st) {
@@ -255,6 +257,7 @@ extern "C" void ctprj_batch_destroy(ctprj_batch *b)
     cudaFree(b->d_bprefix);
     cudaFree(b->d_tprefix);
     cudaFree(b->d_counter);
+    cudaFree(b->d_status);
     delete b;
 }
 
@@ -417,4 +420,60 @@ extern "C" int ctprj_batch_autotune(ctprj_batch *b, void *stream, const char *ca
             fclose(f);
         }
     return cuda_error(cudaGetLastError(), "autotune");
+}
+
+// ----------------------------------------------------------------- streaming
+
+extern "C" int ctprj_stream_flags_create(int n, int **host_flags, int **dev_flags)
+{
+    if (n < 1 || !host_flags || !dev_flags) return set_error(CTPRJ_EINVAL, "invalid arguments");
+    int *h = nullptr;
+    int st = cuda_error(cudaHostAlloc((void **)&h, sizeof(int) * n, cudaHostAllocMapped), "flag allocation");
+    if (st) return st;
+    memset(h, 0, sizeof(int) * n);
+    int *d = nullptr;
+    if ((st = cuda_error(cudaHostGetDevicePointer((void **)&d, h, 0), "flag mapping"))) {
+        cudaFreeHost(h);
+        return st;
+    }
+    *host_flags = h;
+    *dev_flags = d;
+    return CTPRJ_OK;
+}
+
+extern "C" void ctprj_stream_flags_destroy(int *host_flags)
+{
+    if (host_flags) cudaFreeHost(host_flags);
+}
+
+extern "C" int ctprj_batch_stream_backward(ctprj_batch *b, const int *dev_flags, double timeout_s,
+                                           int *status, void *stream)
+{
+    if (!b || !(b->bound & 2) || !dev_flags)
+        return set_error(CTPRJ_EINVAL, "batch has no backward buffers bound or no flags");
+    if (!(timeout_s > 0) || timeout_s > 60)
+        return set_error(CTPRJ_EINVAL, "timeout must be in (0, 60] seconds");
+    Dev dv(b->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    int st;
+    if ((st = cuda_error(cudaMemsetAsync(b->d_counter + 1, 0, sizeof(unsigned long long), s), "batch counter")) ||
+        (st = cuda_error(cudaMemsetAsync(b->d_status, 0, sizeof(int) * b->n, s), "stream status")))
+        return st;
+    const int seg = b->seg <= 32 ? 32 : 64;
+    const int vb = seg == 32 ? b->cfg.bwd_vb : 8;
+    if ((st = launch_backward_stream(bwd_args(b), seg, vb, ctas(b, 1, bwd_param(b), b->cfg.bwd_occ),
+                                     dev_flags, b->d_status,
+                                     (unsigned long long)(timeout_s * 1e9), s)))
+        return st;
+    std::vector<int> h(b->n, 0);
+    if ((st = cuda_error(cudaMemcpyAsync(h.data(), b->d_status, sizeof(int) * b->n, cudaMemcpyDeviceToHost, s), "stream status")) ||
+        (st = cuda_error(cudaStreamSynchronize(s), "stream synchronize")))
+        return st;
+    int late = 0;
+    for (int i = 0; i < b->n; ++i) {
+        if (status) status[i] = h[i];
+        late += h[i] != 0;
+    }
+    if (late) return set_error(CTPRJ_ETIMEOUT, "%d of %d slices were not published within %.3g s", late, b->n, timeout_s);
+    return CTPRJ_OK;
 }

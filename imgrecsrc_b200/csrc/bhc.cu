@@ -15,17 +15,6 @@
 #include "ctprj_internal.h"
 #include "bhc_spline.cuh"
 
-struct ctprj_bhc {
-    ctprj_plan *plan;
-    int J;
-    double Ts;
-    double *d_tab;       // J * kSplStride
-    float *d_s, *d_r, *d_w;   // per-ray state, np * prjWidth each
-    double *d_part;      // per-block partials
-    int part_cap;        // doubles in d_part
-    int saved;           // the per-ray state holds the last forward's values
-};
-
 namespace ctprj {
 
 constexpr int kSpecThreads = 256;
@@ -221,20 +210,6 @@ static int ensure_parts(ctprj_bhc *m, int need)
     if (!st) m->part_cap = need;
     return st;
 }
-
-struct PlanDevice {
-    int prev = -1;
-    int dev;
-    explicit PlanDevice(int d) : dev(d)
-    {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~PlanDevice()
-    {
-        if (prev >= 0 && prev != dev) cudaSetDevice(prev);
-    }
-};
 
 extern "C" int ctprj_bhc_create(ctprj_plan *plan, int J, const double *kappa_nodes, double Ts,
                                 ctprj_bhc **out)

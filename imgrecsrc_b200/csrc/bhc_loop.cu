@@ -1,0 +1,686 @@
+// bhc_loop.cu -- the alternating beam-hardening reconstruction loop.
+//
+// The reference alternates an image step and a spectrum step
+// (bhc/beamhardenSpline.m:340-570): the image step minimises the Poisson
+// likelihood in the density with Nesterov's proximal gradient method (NPG,
+// npg/NPG.m), the spectrum step updates the B-spline coefficients Ie >= 0 on
+// poissLI's objective (bhc/poissLI.m:2-16).  This file runs that loop on the
+// GPU:
+//
+//  density step   one NPG iteration: extrapolation, the fused forward and its
+//                 adjoint at xbar, a majorisation line search on the fused
+//                 forward, momentum restart (ctprj_bhc_reconstruct below);
+//  spectrum step  Newton on Ie >= 0: gradient A^T (1 - m/Ir) and Hessian
+//                 A^T diag(m / Ir^2) A reduced in FP64 from the rays x J basis
+//                 matrix A of the current projections, the quadratic model
+//                 minimised over Ie >= 0 by an active-set method in one warp
+//                 (FP64 Cholesky, diagonal lifted until positive definite as
+//                 bhc/ActiveSet.m:62-76 lifts the eigenvalues), then a line
+//                 search shrinking the step by 0.8 (ActiveSet stepShrnk).
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ctprj_internal.h"
+#include "bhc_spline.cuh"
+#include "../../include/ctprj_bhc_loop.h"
+
+namespace ctprj {
+
+constexpr int kIeChunk = 64;          // rays per shared-memory chunk
+constexpr int kIeThreads = 256;
+constexpr int kMaxH = kMaxJ * (kMaxJ + 1) / 2;
+
+// per-block partials of f, g (J) and the upper triangle of H (J(J+1)/2) for
+// Ie; layout part[block * (1 + J + J(J+1)/2)]
+__global__ void __launch_bounds__(kIeThreads)
+k_ie_eval(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
+          const double *__restrict__ Ie, int want_h, double *__restrict__ part)
+{
+    __shared__ double As[kIeChunk][kMaxJ];
+    __shared__ double rs[kIeChunk], ds[kIeChunk], fs[kIeChunk];
+    __shared__ double Is[kMaxJ];
+    const int nh = J * (J + 1) / 2;
+    for (int j = threadIdx.x; j < J; j += blockDim.x) Is[j] = Ie[j];
+    double f = 0.0, g = 0.0;
+    // entries of H owned by this thread: threadIdx.x + q * blockDim.x, q < 3
+    // (J(J+1)/2 <= 528 entries for J <= 32)
+    double h[3] = {0.0, 0.0, 0.0};
+    int hj[3] = {-1, -1, -1}, hk[3] = {-1, -1, -1};
+    for (int q = 0; q < 3; ++q) {
+        const int e = threadIdx.x + q * blockDim.x;
+        if (e >= nh) break;
+        int j = 0, rem = e;
+        while (rem >= J - j) { rem -= J - j; ++j; }
+        hj[q] = j;
+        hk[q] = j + rem;
+    }
+    __syncthreads();
+    for (long long c0 = (long long)blockIdx.x * kIeChunk; c0 < nrays; c0 += (long long)gridDim.x * kIeChunk) {
+        const int nc = (int)(nrays - c0 < kIeChunk ? nrays - c0 : kIeChunk);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nc * J; e += blockDim.x)
+            As[e / J][e % J] = A[(size_t)(c0 + e / J) * J + e % J];
+        __syncthreads();
+        if (threadIdx.x < nc) {
+            double Ir = 0.0;
+            for (int j = 0; j < J; ++j) Ir = fma(As[threadIdx.x][j], Is[j], Ir);
+            const double mi = (double)m[c0 + threadIdx.x];
+            rs[threadIdx.x] = 1.0 - mi / Ir;
+            ds[threadIdx.x] = mi / (Ir * Ir);
+            fs[threadIdx.x] = poisson_term(Ir, mi);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int i = 0; i < nc; ++i) f += fs[i];
+        if (threadIdx.x < J)
+            for (int i = 0; i < nc; ++i) g = fma(As[i][threadIdx.x], rs[i], g);
+        if (want_h) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                if (hj[q] >= 0)
+                    for (int i = 0; i < nc; ++i) h[q] = fma(As[i][hj[q]] * As[i][hk[q]], ds[i], h[q]);
+        }
+    }
+    const int w = 1 + J + nh;
+    double *out = part + (size_t)blockIdx.x * w;
+    if (threadIdx.x == 0) out[0] = f;
+    if (threadIdx.x < J) out[1 + threadIdx.x] = g;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        if (hj[q] >= 0) out[1 + J + threadIdx.x + q * blockDim.x] = want_h ? h[q] : 0.0;
+}
+
+// out[c] = sum over blocks of part[b * stride + c] for c < ncols (fixed order, FP64)
+__global__ void k_ie_sum(const double *__restrict__ part, int nblocks, int stride, int ncols,
+                         double *__restrict__ out)
+{
+    for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+        double t = 0.0;
+        for (int b = 0; b < nblocks; ++b) t += part[(size_t)b * stride + c];
+        out[c] = t;
+    }
+}
+
+// The Newton direction of the spectrum step.  The quadratic model
+//   q(y) = 1/2 y'Hy + c'y,   c = g - H Ie,
+// is minimised over y >= 0 by a primal active-set method started at y = Ie
+// (working set W: coefficients held at 0); dir = y - Ie, a feasible direction
+// along which the line search needs no projection.  The reference's
+// ActiveSet class (bhc/ActiveSet.m:52-181) also keeps the iterate feasible and
+// moves the active set one constraint at a time; here the subproblem is solved
+// to its optimum every Newton step, which is what makes the outer iteration
+// converge in a few steps although H spans many decades.
+// On each free set F, H_FF z_F = -c_F is solved by a Cholesky factorisation of
+// the Jacobi-scaled block (unit diagonal), the diagonal lifted until every
+// pivot stays above 1e-14 (bhc/ActiveSet.m:62-76 lifts the eigenvalues of the
+// reduced Hessian the same way).  A full step to z ends in a multiplier check
+// (release the most negative lambda_j = (Hy + c)_j of W); a blocked step adds
+// the blocking coefficient to W.
+// One warp: lane t owns coefficient t; inside a factorisation lane r owns row
+// r of the free block.  All branches that end loops are warp-uniform.
+__global__ void __launch_bounds__(32)
+k_ie_qp(const double *__restrict__ fgh, const double *__restrict__ Ie, int J, double *__restrict__ dir,
+        int *__restrict__ qp_iters)
+{
+    __shared__ double H[kMaxJ][kMaxJ + 1];
+    __shared__ double L[kMaxJ][kMaxJ + 1];
+    __shared__ double rhs[kMaxJ], ys[kMaxJ], cs[kMaxJ], dgs[kMaxJ];
+    __shared__ int Fidx[kMaxJ];
+    const unsigned full = 0xffffffffu;
+    const int t = threadIdx.x;
+    const double *g = fgh + 1, *hp = fgh + 1 + J;
+    if (t < J)
+        for (int k = t; k < J; ++k) {
+            const double v = hp[t * J - t * (t - 1) / 2 + (k - t)];   // packed upper triangle
+            H[t][k] = v;
+            H[k][t] = v;
+        }
+    __syncwarp();
+    // a coefficient whose basis function vanishes on every ray has H_tt = 0
+    // (and a zero row): it is left where it is
+    const bool fixed = !(t < J) || !(H[t < J ? t : 0][t < J ? t : 0] > 0.0);
+    const double ie = t < J ? Ie[t] : 0.0;
+    const double dg = fixed ? 1.0 : sqrt(H[t][t]);
+    double c = 0.0;
+    if (t < J) {
+        double hy = 0.0;
+        for (int k = 0; k < J; ++k) hy = fma(H[t][k], Ie[k], hy);
+        c = g[t] - hy;
+    }
+    double y = fixed ? ie : fmax(ie, 0.0);
+    bool inW = !fixed && !(ie > 0.0);
+    cs[t] = c;
+    dgs[t] = dg;
+    int it = 0;
+    for (; it < 8 * J + 16; ++it) {
+        const bool fr = !fixed && !inW;
+        const unsigned fm = __ballot_sync(full, fr);
+        const int nf = __popc(fm);
+        if (fr) Fidx[__popc(fm & ((1u << t) - 1u))] = t;
+        __syncwarp();
+        double z = y;
+        bool solved = true;
+        if (nf > 0) {
+            const int r = t;   // row owned in the factorisation
+            const int jr = r < nf ? Fidx[r] : 0;
+            double lift = 0.0;
+            bool ok = false;
+            for (int attempt = 0; attempt < 40 && !ok; ++attempt) {
+                if (r < nf)
+                    for (int b = 0; b <= r; ++b) {
+                        const int jb = Fidx[b];
+                        L[r][b] = H[jr][jb] / (dgs[jr] * dgs[jb]) + (b == r ? lift : 0.0);
+                    }
+                ok = true;
+                for (int k = 0; k < nf; ++k) {
+                    __syncwarp();
+                    const double d = L[k][k];
+                    if (!(d > 1e-14 * (1.0 + lift))) { ok = false; break; }
+                    const double lk = sqrt(d);
+                    __syncwarp();
+                    if (r == k) L[k][k] = lk;
+                    if (r > k && r < nf) L[r][k] /= lk;
+                    __syncwarp();
+                    if (r > k && r < nf) {
+                        const double lrk = L[r][k];
+                        for (int b = k + 1; b <= r; ++b) L[r][b] = fma(-lrk, L[b][k], L[r][b]);
+                    }
+                }
+                __syncwarp();
+                if (!ok) lift = lift == 0.0 ? 1e-14 : lift * 10.0;
+            }
+            if (!ok) {
+                solved = false;
+            } else {
+                if (r < nf) rhs[r] = -cs[jr] / dgs[jr];
+                for (int k = 0; k < nf; ++k) {   // L w = rhs
+                    __syncwarp();
+                    const double wk = rhs[k] / L[k][k];
+                    __syncwarp();
+                    if (r == k) rhs[k] = wk;
+                    if (r > k && r < nf) rhs[r] = fma(-L[r][k], wk, rhs[r]);
+                }
+                for (int k = nf - 1; k >= 0; --k) {   // L^T v = w
+                    __syncwarp();
+                    const double vk = rhs[k] / L[k][k];
+                    __syncwarp();
+                    if (r == k) rhs[k] = vk;
+                    if (r < k) rhs[r] = fma(-L[k][r], vk, rhs[r]);
+                }
+                __syncwarp();
+                if (fr) z = rhs[__popc(fm & ((1u << t) - 1u))] / dg;
+            }
+        }
+        if (!solved) break;
+        const double p = fr ? z - y : 0.0;
+        // ratio test: the first coefficient to reach 0 along p
+        double rv = (fr && p < 0.0) ? -y / p : INFINITY;
+        int ri = t;
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(full, rv, o);
+            const int oi = __shfl_xor_sync(full, ri, o);
+            if (ov < rv || (ov == rv && oi < ri)) { rv = ov; ri = oi; }
+        }
+        if (rv >= 1.0) {
+            if (fr) y = z;
+            ys[t] = y;
+            __syncwarp();
+            double hy = 0.0;
+            if (t < J)
+                for (int k = 0; k < J; ++k) hy = fma(H[t][k], ys[k], hy);
+            const double lam = hy + c;
+            const bool cand = inW && lam < -1e-13 * (fabs(c) + fabs(hy));
+            if (__ballot_sync(full, cand) == 0u) { ++it; break; }   // optimal
+            double lv = cand ? lam : INFINITY;
+            int li = t;
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(full, lv, o);
+                const int oi = __shfl_xor_sync(full, li, o);
+                if (ov < lv || (ov == lv && oi < li)) { lv = ov; li = oi; }
+            }
+            if (t == li) inW = false;
+        } else {
+            if (fr) y = fma(rv, p, y);
+            if (t == ri) {
+                y = 0.0;
+                inW = true;
+            }
+        }
+        __syncwarp();
+    }
+    if (t < J) dir[t] = y - ie;
+    if (t == 0 && qp_iters) *qp_iters = it;
+}
+
+// Ie_trial = max(0, Ie + step * dir); out[J] = g . (Ie_trial - Ie)
+__global__ void k_ie_trial(const double *__restrict__ Ie, const double *__restrict__ dir,
+                           const double *__restrict__ fgh, int J, double step,
+                           double *__restrict__ trial)
+{
+    if (threadIdx.x == 0) {
+        double gd = 0.0;
+        for (int j = 0; j < J; ++j) {
+            const double v = fmax(0.0, Ie[j] + step * dir[j]);
+            trial[j] = v;
+            gd += fgh[1 + j] * (v - Ie[j]);
+        }
+        trial[J] = gd;
+    }
+}
+
+// x_new = max(0, x - a g); per-block partials of g . (x_new - x) and |x_new - x|^2
+__global__ void __launch_bounds__(256)
+k_pg_step(const float *__restrict__ x, const float *__restrict__ g, long long n, float a,
+          float *__restrict__ xn, double *__restrict__ part)
+{
+    __shared__ double red[2][8];
+    double gd = 0.0, dd = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float v = fmaxf(0.0f, x[i] - a * g[i]);
+        xn[i] = v;
+        const double d = (double)v - (double)x[i];
+        gd = fma((double)g[i], d, gd);
+        dd = fma(d, d, dd);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        gd += __shfl_down_sync(0xffffffffu, gd, o);
+        dd += __shfl_down_sync(0xffffffffu, dd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = gd;
+        red[1][threadIdx.x >> 5] = dd;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a0 += red[0][w];
+            a1 += red[1][w];
+        }
+        part[2 * blockIdx.x] = a0;
+        part[2 * blockIdx.x + 1] = a1;
+    }
+}
+
+// Nesterov extrapolation xbar = max(0, x + coef (x - xprev)); per-block
+// partials of sum |xbar - x| (whether the step carries momentum)
+__global__ void __launch_bounds__(256)
+k_npg_extrapolate(const float *__restrict__ x, const float *__restrict__ xprev, long long n, float coef,
+                  float *__restrict__ xbar, double *__restrict__ part)
+{
+    __shared__ double red[8];
+    double mom = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float xi = x[i];
+        const float v = fmaxf(0.0f, fmaf(coef, xi - xprev[i], xi));
+        xbar[i] = v;
+        mom += fabs((double)v - (double)xi);
+    }
+    for (int o = 16; o > 0; o >>= 1) mom += __shfl_down_sync(0xffffffffu, mom, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mom;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) a += red[w];
+        part[2 * blockIdx.x] = a;
+        part[2 * blockIdx.x + 1] = 0.0;
+    }
+}
+
+// basis matrix from the saved per-ray projections s (already scaled by Ts)
+__global__ void __launch_bounds__(256)
+k_basis_from_s(const float *__restrict__ s, long long nrays, const double *__restrict__ tab_g, int J,
+               double *__restrict__ A)
+{
+    __shared__ double tab[kMaxJ * kSplStride];
+    for (int i = threadIdx.x; i < J * kSplStride; i += blockDim.x) tab[i] = tab_g[i];
+    __syncthreads();
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double si = (double)s[i];
+        const double is2 = 1.0 / (si * si), as = fabs(si);
+        double eL = exp(-tab[0] * si), eC = exp(-tab[1] * si);
+        double *row = A + (size_t)i * J;
+        for (int j = 0; j < J; ++j) {
+            const double *t = tab + j * kSplStride;
+            const double eR = exp(-t[2] * si);
+            double bj = ((eC - eR) * t[4] - (eL - eC) * t[3]) * is2;
+            if (as < t[9]) bj = fma(fma(fma(t[8], si, t[7]), si, t[6]), si, t[5]);
+            row[j] = bj;
+            eL = eC;
+            eC = eR;
+        }
+    }
+}
+
+}  // namespace ctprj
+
+using namespace ctprj;
+
+namespace {
+
+// device scratch of the spectrum step: the rays x J basis matrix and the
+// reduction buffers
+struct SpectrumWs {
+    double *A = nullptr, *part = nullptr, *fgh = nullptr, *dir = nullptr, *trial = nullptr, *f1 = nullptr;
+    int *qp_iters = nullptr;
+    int blocks = 0;
+    int alloc(int J, long long nr, int nblocks, cudaStream_t s)
+    {
+        const int w = 1 + J + J * (J + 1) / 2;
+        blocks = nblocks;
+        int st;
+        if ((st = cuda_error(cudaMallocAsync((void **)&A, sizeof(double) * nr * J, s), "basis matrix")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&part, sizeof(double) * nblocks * w, s), "partials")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&fgh, sizeof(double) * w, s), "partials")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&dir, sizeof(double) * J, s), "partials")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&trial, sizeof(double) * (J + 1), s), "partials")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&f1, sizeof(double) * 2, s), "partials")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&qp_iters, sizeof(int), s), "partials")))
+            release(s);
+        return st;
+    }
+    void release(cudaStream_t s)
+    {
+        if (A) cudaFreeAsync(A, s);
+        if (part) cudaFreeAsync(part, s);
+        if (fgh) cudaFreeAsync(fgh, s);
+        if (dir) cudaFreeAsync(dir, s);
+        if (trial) cudaFreeAsync(trial, s);
+        if (f1) cudaFreeAsync(f1, s);
+        if (qp_iters) cudaFreeAsync(qp_iters, s);
+        A = part = fgh = dir = trial = f1 = nullptr;
+        qp_iters = nullptr;
+    }
+};
+
+int sm_count(int dev)
+{
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+template <class T>
+int fetch(T *h, const T *d, size_t n, cudaStream_t s)
+{
+    int st = cuda_error(cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, s), "readback");
+    if (st) return st;
+    return cuda_error(cudaStreamSynchronize(s), "readback sync");
+}
+
+// Newton steps on Ie >= 0 over the saved projections m->d_s: model f, g, H
+// (k_ie_eval), the QP direction (k_ie_qp), then a backtracking line search
+// along the feasible direction, step x0.8 (bhc/ActiveSet.m stepShrnk), until
+// f(Ie + a d) <= f + 1e-4 g.(a d).  Stops early when g.d >= -1e-14 |f| (the
+// model predicts no decrease) or no step decreases f.  *f_out: f at the
+// returned Ie.
+int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_steps, double *f_out,
+                   SpectrumWs &ws, int *steps_done, cudaStream_t s)
+{
+    const int J = m->J, w = 1 + J + J * (J + 1) / 2;
+    const long long nr = (long long)m->plan->g.np * m->plan->g.W;
+    const int dev = m->plan->device;
+    k_basis_from_s<<<4 * sm_count(dev), 256, 0, s>>>(m->d_s, nr, m->d_tab, J, ws.A);
+    int st = cuda_error(cudaGetLastError(), "basis matrix");
+    double fcur = 0.0;
+    int done = 0;
+    for (int it = 0; it < newton_steps && !st; ++it) {
+        k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, 1, ws.part);
+        k_ie_sum<<<1, 256, 0, s>>>(ws.part, ws.blocks, w, w, ws.fgh);
+        k_ie_qp<<<1, 32, 0, s>>>(ws.fgh, d_Ie, J, ws.dir, ws.qp_iters);
+        if ((st = cuda_error(cudaGetLastError(), "spectrum Newton"))) break;
+        if ((st = fetch(&fcur, ws.fgh, 1, s))) break;
+        double step = 1.0;
+        bool accepted = false, converged = false;
+        for (int ls = 0; ls < 40; ++ls, step *= 0.8) {
+            k_ie_trial<<<1, 32, 0, s>>>(d_Ie, ws.dir, ws.fgh, J, step, ws.trial);
+            k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, 0, ws.part);
+            k_ie_sum<<<1, 32, 0, s>>>(ws.part, ws.blocks, w, 1, ws.f1);
+            double fn = 0.0, gd = 0.0;
+            if ((st = cuda_error(cudaMemcpyAsync(&fn, ws.f1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
+                (st = fetch(&gd, ws.trial + J, 1, s)))
+                break;
+            if (ls == 0 && !(gd < -1e-14 * fabs(fcur))) {
+                converged = true;
+                break;
+            }
+            if (fn <= fcur + 1e-4 * gd) {
+                st = cuda_error(cudaMemcpyAsync(d_Ie, ws.trial, sizeof(double) * J, cudaMemcpyDeviceToDevice, s), "accept");
+                fcur = fn;
+                accepted = true;
+                break;
+            }
+        }
+        if (!accepted || converged) break;
+        ++done;
+    }
+    if (f_out) *f_out = fcur;
+    if (steps_done) *steps_done = done;
+    return st;
+}
+
+}  // namespace
+
+extern "C" int ctprj_bhc_spectrum_step(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_steps,
+                                       double *f_out, void *stream)
+{
+    if (!m || !d_imea || !d_Ie) return set_error(CTPRJ_EINVAL, "NULL argument");
+    if (!m->saved) return set_error(CTPRJ_EINVAL, "the spectrum step needs a saved forward state");
+    if (newton_steps < 1) return set_error(CTPRJ_EINVAL, "newton_steps must be >= 1");
+    cudaStream_t s = (cudaStream_t)stream;
+    SpectrumWs ws;
+    int st = ws.alloc(m->J, (long long)m->plan->g.np * m->plan->g.W, 2 * sm_count(m->plan->device), s);
+    if (st) return st;
+    st = spectrum_steps(m, d_imea, d_Ie, newton_steps, f_out, ws, nullptr, s);
+    ws.release(s);
+    return st;
+}
+
+namespace {
+
+// the likelihood at (x, Ie), fused or from the plain projection; the per-ray
+// state is saved (the spectrum step and the gradient read it)
+int likelihood(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *d_imea, double *d_f,
+               float *sino, cudaStream_t s)
+{
+    if (!sino) return ctprj_bhc_forward(m, d_x, d_Ie, d_imea, d_f, 1, s);
+    int st = ctprj_forward(m->plan, d_x, sino, s);
+    if (st) return st;
+    return ctprj_bhc_terms(m, sino, d_Ie, d_imea, d_f, 1, s);
+}
+
+struct LoopBufs {
+    float *gx = nullptr, *xn = nullptr, *xbar = nullptr, *xprev = nullptr, *sino = nullptr;
+    double *f = nullptr, *part = nullptr, *sum = nullptr;
+    void release()
+    {
+        cudaFree(gx); cudaFree(xn); cudaFree(xbar); cudaFree(xprev); cudaFree(sino);
+        cudaFree(f); cudaFree(part); cudaFree(sum);
+    }
+};
+
+}  // namespace
+
+// The density step follows the reference's NPG class (npg/NPG.m main, with
+// the proximal map reduced to the projection on x >= 0):
+//   theta' = (1 + sqrt(1 + 4 theta^2)) / 2,  xbar = max(0, x + (theta-1)/theta' (x - xprev));
+//   f, grad at xbar;  candidate xn = max(0, xbar - grad / t), accepted when
+//   f(xn) <= f(xbar) + grad.(xn - xbar) + t/2 |xn - xbar|^2 (utils/Utils.m
+//   majorizationHolds); on failure t /= 0.5 (at most 20 times); in the first
+//   10 iterations a success is retried with t *= 0.5 while it holds (at most
+//   17 times); after 4 consecutive first-try successes t *= 0.5 once (failure
+//   of that try raises the count needed by 4);
+//   if f(xn) exceeds the cost of the previous iteration: restart without
+//   momentum (theta = 1) when xbar != x, else keep x (the reference's further
+//   retries with tighter inner ADMM tolerances do not apply to an exact
+//   projection).
+// Then the spectrum step on the accepted density's projections, whose f
+// becomes the cost the next density step compares against
+// (bhc/beamhardenSpline.m:382-470).
+extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, const float *d_imea,
+                                     const ctprj_bhc_loop_opts *opts, ctprj_bhc_loop_stats *stats,
+                                     void *stream)
+{
+    if (!m || !d_x || !d_Ie || !d_imea || !opts) return set_error(CTPRJ_EINVAL, "NULL argument");
+    if (opts->iterations < 0) return set_error(CTPRJ_EINVAL, "negative iteration count");
+    PlanDevice pd(m->plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long npx = (long long)m->plan->g.n * m->plan->g.n;
+    const long long nr = (long long)m->plan->g.np * m->plan->g.W;
+    const int dev = m->plan->device;
+    const int pgb = 2 * sm_count(dev);
+    LoopBufs b;
+    SpectrumWs ws;
+    int st;
+    if ((st = cuda_error(cudaMalloc((void **)&b.gx, sizeof(float) * npx), "loop buffers")) ||
+        (st = cuda_error(cudaMalloc((void **)&b.xn, sizeof(float) * npx), "loop buffers")) ||
+        (st = cuda_error(cudaMalloc((void **)&b.xbar, sizeof(float) * npx), "loop buffers")) ||
+        (st = cuda_error(cudaMalloc((void **)&b.xprev, sizeof(float) * npx), "loop buffers")) ||
+        (st = cuda_error(cudaMalloc((void **)&b.f, sizeof(double) * 2), "loop buffers")) ||
+        (st = cuda_error(cudaMalloc((void **)&b.part, sizeof(double) * 2 * pgb), "loop buffers")) ||
+        (st = cuda_error(cudaMalloc((void **)&b.sum, sizeof(double) * 2), "loop buffers")) ||
+        (opts->unfused &&
+         (st = cuda_error(cudaMalloc((void **)&b.sino, sizeof(float) * nr), "loop buffers"))) ||
+        (!opts->skip_spectrum && (st = ws.alloc(m->J, nr, pgb, s)))) {
+        b.release();
+        return st;
+    }
+    const int newton = opts->spectrum_newton_steps > 0 ? opts->spectrum_newton_steps : 2;
+    double t = 1.0 / (opts->x_step > 0 ? opts->x_step : 1.0);   // inverse step size
+    double theta = 0.0, cost = INFINITY;
+    int p = 0, cumu = 0, cumu_tol = 4, evals = 0, restarts = 0, newton_done = 0;
+    const int pre_steps = 10;
+    const double shrink = 0.5;
+    float ms_spec = 0.0f;
+    cudaEvent_t e0, e1, es0, es1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&es0);
+    cudaEventCreate(&es1);
+    st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "loop start");
+    cudaEventRecord(e0, s);
+    int done = 0;
+    for (int it = 0; it < opts->iterations && !st; ++it) {
+        double nc = 0.0;
+        bool moved = false, state_at_x = false;
+        for (int pass = 0; pass < 3 && !st; ++pass) {
+            ++p;
+            const double theta1 = (1.0 + sqrt(1.0 + 4.0 * theta * theta)) / 2.0;
+            const float coef = (float)((theta - 1.0) / theta1);
+            k_npg_extrapolate<<<pgb, 256, 0, s>>>(d_x, b.xprev, npx, coef, b.xbar, b.part);
+            k_ie_sum<<<1, 32, 0, s>>>(b.part, pgb, 2, 1, b.sum + 1);
+            double f0 = 0.0, mom = 0.0;
+            if ((st = cuda_error(cudaGetLastError(), "extrapolation")) ||
+                (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, b.sino, s)) ||
+                (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.gx, nullptr, s)) ||
+                (st = cuda_error(cudaMemcpyAsync(&mom, b.sum + 1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
+                (st = fetch(&f0, b.f, 1, s)))
+                break;
+            ++evals;
+            int ppp = 0;
+            bool good = true, inc = false, good_mm = true;
+            if (cumu >= cumu_tol) {   // adaptively grow the step
+                t *= shrink;
+                cumu = 0;
+                inc = true;
+            }
+            while (true) {
+                ++ppp;
+                k_pg_step<<<pgb, 256, 0, s>>>(b.xbar, b.gx, npx, (float)(1.0 / t), b.xn, b.part);
+                k_ie_sum<<<1, 32, 0, s>>>(b.part, pgb, 2, 2, b.sum);
+                double gd_dd[2];
+                if ((st = cuda_error(cudaGetLastError(), "density step")) ||
+                    (st = likelihood(m, b.xn, d_Ie, d_imea, b.f + 1, b.sino, s)) ||
+                    (st = cuda_error(cudaMemcpyAsync(gd_dd, b.sum, 2 * sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
+                    (st = fetch(&nc, b.f + 1, 1, s)))
+                    break;
+                ++evals;
+                if (nc - f0 <= gd_dd[0] + 0.5 * t * gd_dd[1]) {
+                    if (p <= pre_steps && ppp < 18 && good) {
+                        t *= shrink;
+                        continue;
+                    }
+                    break;
+                }
+                if (ppp <= 20) {
+                    t /= shrink;
+                    good = false;
+                    if (inc) {
+                        cumu_tol += 4;
+                        inc = false;
+                    }
+                } else {
+                    good_mm = false;
+                    break;
+                }
+            }
+            if (st) break;
+            if (nc > cost) {
+                if (good_mm && mom != 0.0 && pass < 2) {   // restart without momentum
+                    theta = 1.0;
+                    ++restarts;
+                    continue;
+                }
+                nc = cost;   // keep x
+                moved = false;
+            } else {
+                moved = true;
+            }
+            theta = theta1;
+            st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "accept");
+            if (!st && moved)
+                st = cuda_error(cudaMemcpyAsync(d_x, b.xn, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "accept");
+            state_at_x = moved;   // the last likelihood evaluated (and saved) was at xn
+            cumu = ppp == 1 ? cumu + 1 : 0;
+            break;
+        }
+        if (st) break;
+        cost = nc;
+        if (stats && it < CTPRJ_BHC_LOOP_MAX_TRACE) stats->x_step[it] = moved ? 1.0 / t : 0.0;
+        if (!opts->skip_spectrum) {
+            cudaEventRecord(es0, s);
+            if (!state_at_x) {
+                if ((st = likelihood(m, d_x, d_Ie, d_imea, b.f, b.sino, s))) break;
+                ++evals;
+            }
+            double fs = 0.0;
+            int nd = 0;
+            if ((st = spectrum_steps(m, d_imea, d_Ie, newton, &fs, ws, &nd, s))) break;
+            newton_done += nd;
+            cudaEventRecord(es1, s);
+            cudaEventSynchronize(es1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, es0, es1);
+            ms_spec += ms;
+            cost = fs;
+        }
+        if (stats && it < CTPRJ_BHC_LOOP_MAX_TRACE) stats->cost[it] = cost;
+        done = it + 1;
+    }
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(es0);
+    cudaEventDestroy(es1);
+    if (stats) {
+        stats->iterations = done;
+        stats->final_cost = cost;
+        stats->final_x_step = 1.0 / t;
+        stats->ms = ms;
+        stats->ms_spectrum = ms_spec;
+        stats->evaluations = evals;
+        stats->restarts = restarts;
+        stats->newton_steps = newton_done;
+    }
+    ws.release(s);
+    cudaStreamSynchronize(s);
+    b.release();
+    return st;
+}

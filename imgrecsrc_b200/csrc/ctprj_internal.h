@@ -129,7 +129,34 @@ struct ctprj_plan {
     float *d_fsino;
 };
 
+// polychromatic model on a plan (bhc.cu, bhc_loop.cu)
+struct ctprj_bhc {
+    ctprj_plan *plan;
+    int J;
+    double Ts;
+    double *d_tab;            // spline table, J * kSplStride doubles
+    float *d_s, *d_r, *d_w;   // per-ray state, np * prjWidth each
+    double *d_part;           // per-block partials
+    int part_cap;             // doubles in d_part
+    int saved;                // the per-ray state holds the last forward's values
+};
+
 namespace ctprj {
+
+// makes a plan's device current for the lifetime of the guard
+struct PlanDevice {
+    int prev = -1;
+    int dev;
+    explicit PlanDevice(int d) : dev(d)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~PlanDevice()
+    {
+        if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    }
+};
 
 int set_error(int status, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
@@ -151,6 +178,8 @@ int launch_transpose_batch(const BatchArgs &a, cudaStream_t s);
 int launch_forward_batch(const BatchArgs &a, int views, int ctas, cudaStream_t s);
 int launch_backward_batch(const BatchArgs &a, int seg, int vb, int ctas, cudaStream_t s);
 int batch_max_ctas(int kind, int param, int *per_sm);
+int launch_backward_stream(const BatchArgs &a, int seg, int vb, int ctas, const int *ready,
+                           int *status, unsigned long long timeout_ns, cudaStream_t s);
 int launch_backward(const ctprj_plan *p, const float *sino, float *img, int fbp,
                     unsigned long long *counter, cudaStream_t s, float scale = 1.0f);
 

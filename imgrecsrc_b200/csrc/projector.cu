@@ -30,11 +30,19 @@
 
 namespace ctprj {
 
-constexpr int kFwdThreads = 128;
 // a forward block is kFwdViews adjacent base views x 32 adjacent rays, one view
 // per warp: the warps march over nearly the same image lines at the same time,
-// so the rows they gather are shared in L1
-constexpr int kFwdViews = kFwdThreads / 32;
+// so the rows they gather are shared in L1.  CTPRJ_FWD_VIEWS and
+// CTPRJ_FWD_MINBLOCKS (resident blocks asked of the register allocator) are
+// build-time launch-shape choices.
+#ifndef CTPRJ_FWD_VIEWS
+#define CTPRJ_FWD_VIEWS 4
+#endif
+#ifndef CTPRJ_FWD_MINBLOCKS
+#define CTPRJ_FWD_MINBLOCKS 1
+#endif
+constexpr int kFwdViews = CTPRJ_FWD_VIEWS;
+constexpr int kFwdThreads = 32 * kFwdViews;
 constexpr int kBwdTile = 16;   // 16 x 16 octant pixels per block
 
 // --------------------------------------------------------------- transpose
@@ -252,7 +260,7 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
 }
 
 template <bool FAN, int MODE>
-__global__ void __launch_bounds__(kFwdThreads)
+__global__ void __launch_bounds__(kFwdThreads, CTPRJ_FWD_MINBLOCKS)
 k_forward(const FwdParams p, const float *__restrict__ img, const float *__restrict__ imgT,
           float *__restrict__ sino, unsigned long long *__restrict__ counter)
 {
@@ -915,6 +923,85 @@ __global__ void __launch_bounds__(kBwdTile * kBwdTile, 4) k_backward_batch(const
             else backward_tile_direct<false>(sl.bp, tile, sl.bsino, sl.bimg);
         }
     }
+}
+
+// ------------------------------------------------- streaming backprojection
+//
+// A persistent backprojection whose inputs arrive while it runs: the host
+// publishes slice i by setting ready[i] != 0 in host-mapped memory once its
+// sinogram is on the device.  A block that takes a tile of slice i waits for
+// that flag -- polling with __nanosleep -- for at most timeout_ns of
+// %globaltimer time; past it, the slice is marked timed out (status[i] = 1),
+// its remaining tiles are skipped by every block, and the host reports
+// CTPRJ_ETIMEOUT.  No wait is unbounded and nothing traps, so the context stays
+// usable after a timeout.
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <int SEG, int VB>
+__global__ void __launch_bounds__(kBwdTile * kBwdTile, 4)
+k_backward_stream(const BatchArgs a, const volatile int *__restrict__ ready,
+                  int *__restrict__ status, unsigned long long timeout_ns)
+{
+    __shared__ __align__(16) unsigned char raw[tiled_smem_bytes<SEG, VB>()];
+    __shared__ long long slot;
+    __shared__ int go;
+    for (;;) {
+        const long long item = next_item(a.counter, &slot);
+        if (item >= a.total) return;
+        const int i = find_slot(a.prefix, a.nslices, item);
+        const int s = a.order[i];
+        if (threadIdx.x == 0) {
+            int ok = 0;
+            if (((volatile int *)status)[s] == 0) {
+                const unsigned long long t0 = global_ns();
+                for (;;) {
+                    if (ready[s]) { ok = 1; break; }
+                    if (((volatile int *)status)[s] != 0) break;
+                    if (global_ns() - t0 > timeout_ns) {
+                        atomicExch(&status[s], 1);
+                        break;
+                    }
+                    __nanosleep(1000);
+                }
+            }
+            go = ok;
+        }
+        __syncthreads();
+        if (!go) continue;
+        __threadfence();   // the sinogram was published before the flag
+        const BatchSlice &sl = a.slices[s];
+        const int tile = (int)(item - a.prefix[i]);
+        const bool fan = sl.bp.g.fan != 0;
+        if (sl.tiled) {
+            if (fan)
+                backward_tile<true, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
+                                                    *reinterpret_cast<TiledSmem<true, SEG, VB> *>(raw));
+            else
+                backward_tile<false, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
+                                                     *reinterpret_cast<TiledSmem<false, SEG, VB> *>(raw));
+        } else {
+            if (fan) backward_tile_direct<true>(sl.bp, tile, sl.bsino, sl.bimg);
+            else backward_tile_direct<false>(sl.bp, tile, sl.bsino, sl.bimg);
+        }
+    }
+}
+
+int launch_backward_stream(const BatchArgs &a, int seg, int vb, int ctas, const int *ready,
+                           int *status, unsigned long long timeout_ns, cudaStream_t s)
+{
+    if (seg <= 32 && vb == 16)
+        k_backward_stream<32, 16><<<ctas, 256, 0, s>>>(a, ready, status, timeout_ns);
+    else if (seg <= 32)
+        k_backward_stream<32, 8><<<ctas, 256, 0, s>>>(a, ready, status, timeout_ns);
+    else
+        k_backward_stream<64, 8><<<ctas, 256, 0, s>>>(a, ready, status, timeout_ns);
+    return cuda_error(cudaGetLastError(), "streaming backward launch");
 }
 
 int launch_transpose_batch(const BatchArgs &a, cudaStream_t s)

@@ -44,6 +44,18 @@ int ctprj_batch_capture(ctprj_batch *batch, void *stream);
  * device and the geometries.  Synchronises `stream`. */
 int ctprj_batch_autotune(ctprj_batch *batch, void *stream, const char *cache_path);
 
+/* Streaming backprojection: the persistent kernel starts before the inputs
+ * exist and backprojects slice i once the host has published it by setting
+ * flag i != 0 (after its sinogram is on the device), in host-mapped flags from
+ * ctprj_stream_flags_create.  A slice not published within timeout_s (at most
+ * 60 s) of a block starting to wait for it is given up: its output is left
+ * untouched, status[i] = 1 (status: nslices ints, may be NULL) and the call
+ * returns CTPRJ_ETIMEOUT; the device stays usable.  Synchronises `stream`. */
+int ctprj_stream_flags_create(int n, int **host_flags, int **dev_flags);
+void ctprj_stream_flags_destroy(int *host_flags);
+int ctprj_batch_stream_backward(ctprj_batch *batch, const int *dev_flags, double timeout_s,
+                                int *status, void *stream);
+
 /* Text of the current launch configuration. */
 int ctprj_batch_config(ctprj_batch *batch, char *buf, int len);
 

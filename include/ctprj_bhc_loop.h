@@ -1,0 +1,71 @@
+/*
+ * ctprj_bhc_loop.h -- the alternating beam-hardening reconstruction on the GPU.
+ *
+ * Counterpart of the reference's BHC driver loop (bhc/beamhardenSpline.m:
+ * 340-570): one density step on the Poisson likelihood (the reference's NPG
+ * class, npg/NPG.m, with the non-negativity projection as its proximal map),
+ * then a non-negative spectrum step, repeated.  Built on the model of
+ * include/ctprj.h (ctprj_bhc_*): every likelihood and gradient of the density
+ * step comes from the fused forward projection and its adjoint; the spectrum
+ * step is a Newton method on Ie >= 0 whose gradient, Hessian, bound-
+ * constrained quadratic subproblem (active set, J x J Cholesky) and line
+ * search run in FP64 on the GPU (bhc/ActiveSet.m is the reference's
+ * active-set Newton method for the same objective, bhc/poissLI.m).
+ */
+#ifndef CTPRJ_BHC_LOOP_H
+#define CTPRJ_BHC_LOOP_H
+
+#include "ctprj.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CTPRJ_BHC_LOOP_MAX_TRACE 256
+
+typedef struct {
+    int iterations;             /* alternating iterations */
+    double x_step;              /* initial density step 1/t (<= 0: 1) */
+    int spectrum_newton_steps;  /* at most this many Newton steps per spectrum
+                                   update (<= 0: 2); fewer when converged */
+    int skip_spectrum;          /* 1: density steps only */
+    int unfused;                /* 1: every likelihood from the plain forward projection
+                                   plus a separate spectrum-terms kernel (comparison) */
+} ctprj_bhc_loop_opts;
+
+typedef struct {
+    int iterations;                           /* completed */
+    double final_cost;                        /* f after the last step */
+    double final_x_step;                      /* density step 1/t at the end */
+    double cost[CTPRJ_BHC_LOOP_MAX_TRACE];    /* f after each iteration */
+    double x_step[CTPRJ_BHC_LOOP_MAX_TRACE];  /* density step accepted in each
+                                                 iteration (0: x kept) */
+    float ms;                                 /* device time of the loop */
+    float ms_spectrum;                        /* of which spectrum steps */
+    int evaluations;                          /* likelihood evaluations (each one
+                                                 forward projection) */
+    int restarts;                             /* momentum restarts */
+    int newton_steps;                         /* accepted spectrum Newton steps */
+} ctprj_bhc_loop_stats;
+
+/* Spectrum update on the projections of the last forward saved by the model
+ * (ctprj_bhc_forward with save != 0): at most newton_steps (>= 1) Newton steps
+ * on Ie >= 0 (d_Ie: J doubles, updated in place), each minimising the
+ * quadratic model over Ie >= 0 and then backtracking (x0.8) to sufficient
+ * decrease; stops early when the model predicts no decrease.  *f_out receives
+ * f at the returned Ie.  Synchronises `stream`. */
+int ctprj_bhc_spectrum_step(ctprj_bhc *model, const float *d_imea, double *d_Ie, int newton_steps,
+                            double *f_out, void *stream);
+
+/* The alternating loop on density d_x (n*n floats, updated in place) and
+ * spectrum d_Ie (updated in place) for measurement d_imea.  Synchronises
+ * `stream` between steps. */
+int ctprj_bhc_reconstruct(ctprj_bhc *model, float *d_x, double *d_Ie, const float *d_imea,
+                          const ctprj_bhc_loop_opts *opts, ctprj_bhc_loop_stats *stats,
+                          void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTPRJ_BHC_LOOP_H */

@@ -5,8 +5,11 @@ Follows bhc/Spline.m:122-203 (b1Iout: Laplace transforms of the degree-1
 B-spline mass-attenuation basis, with their first and second derivatives and
 the cubic Taylor branch near s = 0), bhc/poissLAlpha.m:1-19 (Poisson negative
 log-likelihood in the density and its gradient through Phi^T),
-bhc/poissLI.m:1-27 (the same in the spectrum coefficients, with the Hessian)
-and the kappa grid rule of bhc/beamhardenSpline.m:137-165.
+bhc/poissLI.m:1-27 (the same in the spectrum coefficients, with the Hessian),
+the Gaussian (log-domain least-squares) pair bhc/gaussLAlpha.m:1-34 and
+bhc/gaussLI.m:1-27, the density Hessians of both (the `hessian` closures of
+poissLAlpha / gaussLAlpha) and the kappa grid rule of
+bhc/beamhardenSpline.m:137-165.
 
 The reference is MATLAB and cannot run here: parity of this restatement is
 unpinned against the reference's own outputs; it is cross-checked against
@@ -125,6 +128,42 @@ def poiss_alpha(imea, Ie, s, k, backproject):
     f = poisson_terms(BL, m).sum()
     w = (1 - m / BL) * sBL
     return f, backproject(w), w
+
+
+def poiss_hessian_weight(imea, Ie, s, k):
+    """Per-ray weight of the density Hessian of poissLAlpha
+    (bhc/poissLAlpha.m:15): (sBL/BL)^2 m + ssBL (1 - m/BL); the Hessian is
+    Phi^T diag(weight) Phi."""
+    BL, sBL, ssBL = b1_iout(k, s, Ie)
+    m = np.asarray(imea, np.float64).ravel()
+    return (sBL / BL) ** 2 * m + ssBL * (1 - m / BL)
+
+
+def gauss_alpha(imea, Ie, s, k, backproject):
+    """bhc/gaussLAlpha.m:1-20: Err = log(BL/m), f = Err'Err/2,
+    grad = backproject(Err sBL / BL); returns (f, grad, per-ray weight)."""
+    BL, sBL, _ = b1_iout(k, s, Ie)
+    m = np.asarray(imea, np.float64).ravel()
+    err = np.log(BL / m)
+    w = err * sBL / BL
+    return 0.5 * err @ err, backproject(w), w
+
+
+def gauss_hessian_weight(imea, Ie, s, k):
+    """bhc/gaussLAlpha.m:18: (1 - Err)(sBL/BL)^2 + Err ssBL/BL."""
+    BL, sBL, ssBL = b1_iout(k, s, Ie)
+    m = np.asarray(imea, np.float64).ravel()
+    err = np.log(BL / m)
+    return (1 - err) * (sBL / BL) ** 2 + err * ssBL / BL
+
+
+def gauss_ie(imea, A, Ie):
+    """bhc/gaussLI.m:1-27: Ir = A Ie, Err = log(Ir/m), f = Err'Err/2,
+    g = A^T (Err / Ir), H = A^T diag((1 - Err) / Ir^2) A."""
+    Ir = A @ np.asarray(Ie, np.float64)
+    m = np.asarray(imea, np.float64).ravel()
+    err = np.log(Ir / m)
+    return 0.5 * err @ err, A.T @ (err / Ir), A.T @ (A * ((1 - err) / Ir ** 2)[:, None])
 
 
 def poiss_ie(imea, A, Ie):

@@ -94,3 +94,43 @@ def test_spectrum_gradient_and_hessian_by_central_differences():
 def test_zero_counts_contribute_bl_only():
     f = B.poisson_terms(np.array([0.5, 0.2]), np.array([0.0, 0.2]))
     assert np.allclose(f, [0.5, 0.0])
+
+
+@pytest.mark.parametrize("noise", ["poisson", "gaussian"])
+def test_density_hessian_weight_by_central_differences(noise):
+    """Phi^T diag(weight) Phi v against differences of the gradient
+    (the hessian closures of bhc/poissLAlpha.m:15-18, bhc/gaussLAlpha.m:18-20)."""
+    A, x, k, Ie, m = _problem(seed=5)
+    alpha = B.poiss_alpha if noise == "poisson" else B.gauss_alpha
+    weight = B.poiss_hessian_weight if noise == "poisson" else B.gauss_hessian_weight
+    bp = lambda w: A.T @ w
+    h_w = weight(m, Ie, A @ x, k)
+    rng = np.random.default_rng(6)
+    for _ in range(6):
+        v = rng.standard_normal(x.size)
+        h = 1e-4 * np.linalg.norm(x) / np.linalg.norm(v)
+        gp = alpha(m, Ie, A @ (x + h * v), k, bp)[1]
+        gm = alpha(m, Ie, A @ (x - h * v), k, bp)[1]
+        Hv = A.T @ (h_w * (A @ v))
+        assert np.linalg.norm((gp - gm) / (2 * h) - Hv) <= 1e-6 * np.linalg.norm(Hv)
+
+
+def test_gaussian_pair_by_central_differences():
+    A, x, k, Ie, m = _problem(seed=7)
+    f = lambda xx: B.gauss_alpha(m, Ie, A @ xx, k, lambda w: A.T @ w)[0]
+    _, g, _ = B.gauss_alpha(m, Ie, A @ x, k, lambda w: A.T @ w)
+    rng = np.random.default_rng(8)
+    for _ in range(6):
+        d = rng.standard_normal(x.size)
+        h = 1e-3 * np.linalg.norm(x) / np.linalg.norm(d)
+        fd = (f(x + h * d) - f(x - h * d)) / (2 * h)
+        assert abs(fd - g @ d) <= 1e-5 * np.linalg.norm(g) * np.linalg.norm(d)
+    Bm, _, _ = B.b1_basis(k, A @ x)
+    _, gI, HI = B.gauss_ie(m, Bm, Ie)
+    for _ in range(6):
+        d = rng.standard_normal(Ie.size)
+        h = 1e-4 * np.linalg.norm(Ie) / np.linalg.norm(d)
+        fp, gp, _ = B.gauss_ie(m, Bm, Ie + h * d)
+        fm, gm, _ = B.gauss_ie(m, Bm, Ie - h * d)
+        assert abs((fp - fm) / (2 * h) - gI @ d) <= 1e-6 * np.linalg.norm(gI) * np.linalg.norm(d)
+        assert np.linalg.norm((gp - gm) / (2 * h) - HI @ d) <= 1e-5 * np.linalg.norm(HI @ d)
