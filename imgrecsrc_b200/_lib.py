@@ -32,7 +32,8 @@ class LoopOpts(ctypes.Structure):
     """ctprj_bhc_loop_opts of include/ctprj_bhc_loop.h."""
     _fields_ = [("iterations", ctypes.c_int), ("x_step", ctypes.c_double),
                 ("spectrum_newton_steps", ctypes.c_int), ("skip_spectrum", ctypes.c_int),
-                ("unfused", ctypes.c_int)]
+                ("unfused", ctypes.c_int), ("init_step", ctypes.c_int),
+                ("density_method", ctypes.c_int)]
 
 
 class LoopStats(ctypes.Structure):
@@ -99,6 +100,8 @@ def lib():
         "ctprj_bhc_terms": ([VP, VP, VP, VP, VP, ctypes.c_int, VP], ctypes.c_int),
         "ctprj_bhc_basis": ([VP, VP, VP, VP], ctypes.c_int),
         "ctprj_bhc_state": ([VP, ctypes.POINTER(VP), ctypes.POINTER(VP), ctypes.POINTER(VP)], ctypes.c_int),
+        "ctprj_bhc_set_noise": ([VP, ctypes.c_int], ctypes.c_int),
+        "ctprj_bhc_hessian": ([VP, VP, VP, VP, VP, VP, VP], ctypes.c_int),
         "parPrjConf": ([VP, VP, VP, ctypes.POINTER(ParConf), ctypes.c_size_t], ctypes.c_int),
         "parPrjThread": ([], ctypes.c_int),
         "parPrjRun": ([], ctypes.c_int),

@@ -47,6 +47,7 @@ class BHCModel:
                                      self.Ts, ctypes.byref(self._m)))
         g = projector.geometry
         self.nrays = g.np * g.prjWidth
+        self.noise = "poisson"
 
     def close(self):
         if self._m:
@@ -97,6 +98,28 @@ class BHCModel:
                                     _stream_handle(stream, pr.device)))
         return out
 
+    def set_noise(self, noise):
+        """'poisson' (bhc/poissLAlpha.m, the default) or 'gaussian'
+        (bhc/gaussLAlpha.m: log-domain least squares)."""
+        code = {"poisson": 0, "gaussian": 1}[noise]
+        check(lib().ctprj_bhc_set_noise(self._m, code))
+        self.noise = noise
+
+    def hessian(self, v, Ie, imea, Hv=True, vHv=True, stream=None):
+        """Density Hessian at the saved forward state applied to v:
+        (Ts A^T (h * Ts A v) as (n, n) float32 or None, v'Hv as a float or None)."""
+        import torch
+        pr = self.projector
+        hv = torch.empty(pr.img_shape, dtype=torch.float32, device=v.device) if Hv else None
+        q = torch.zeros(1, dtype=torch.float64, device=v.device) if vHv else None
+        check(lib().ctprj_bhc_hessian(self._m, _dptr(Ie, self.J, torch.float64),
+                                      _dptr(imea, self.nrays, torch.float32),
+                                      _dev_ptr(v, pr.img_shape, pr.device),
+                                      None if hv is None else _dev_ptr(hv, pr.img_shape, pr.device),
+                                      None if q is None else q.data_ptr(),
+                                      _stream_handle(stream, pr.device)))
+        return hv, (q.item() if q is not None else None)
+
     def backward(self, x=None, Ie=None, imea=None, grad_x=True, grad_Ie=True, stream=None):
         """(df/dx as (n, n) float32, df/dIe as (J,) float64); either may be None
         when not requested.  Recomputes the forward when it saved no state."""
@@ -124,14 +147,18 @@ class BHCModel:
         return f.value
 
     def reconstruct(self, x, Ie, imea, iterations, x_step=1.0, spectrum_newton_steps=2,
-                    skip_spectrum=False, unfused=False, stream=None):
+                    skip_spectrum=False, unfused=False, init_step="fixed", method="npg", stream=None):
         """The alternating density / spectrum loop, x and Ie updated in place.
+        init_step: 'fixed' (first step x_step), 'bb' or 'hessian' (the
+        reference's stepSizeInit rules); method: 'npg' (npg/NPG.m) or 'pg'
+        (npg/PG.m) for the density step.
         Returns a dict with the cost after each iteration, the accepted density
         steps and the device time."""
         import torch
         pr = self.projector
         opts = LoopOpts(int(iterations), float(x_step), int(spectrum_newton_steps),
-                        1 if skip_spectrum else 0, 1 if unfused else 0)
+                        1 if skip_spectrum else 0, 1 if unfused else 0,
+                        {"fixed": 0, "bb": 1, "hessian": 2}[init_step], {"npg": 0, "pg": 1}[method])
         st = LoopStats()
         check(lib().ctprj_bhc_reconstruct(self._m, _dev_ptr(x, pr.img_shape, pr.device),
                                           _dptr(Ie, self.J, torch.float64),

@@ -105,13 +105,13 @@ k_bhc_terms(const float *__restrict__ sino, long long nrays, BhcArgs a)
         const double s = a.Ts * (double)sino[i];
         const SplineEval e = b1_eval(s, tab, Ie, a.J);
         const double m = (double)a.imea[i];
-        const double r = 1.0 - m / e.BL;
+        const RayTerms t = ray_terms(a.noise, e.BL, m);
         if (a.w_out) {
-            a.w_out[i] = (float)(r * e.sBL);
+            a.w_out[i] = (float)(t.r * e.sBL);
             a.s_out[i] = (float)s;
-            a.r_out[i] = (float)r;
+            a.r_out[i] = (float)t.r;
         }
-        f += poisson_term(e.BL, m);
+        f += t.f;
     }
     const double t = block_sum_any(f, red);
     if (threadIdx.x == 0) a.part[blockIdx.x] = t;
@@ -193,6 +193,55 @@ static std::vector<double> spline_table(const double *k, int J)
     return t;
 }
 
+// per basis function: the cubic Taylor coefficients of b_j'' about s = 0 and
+// the |s| below which they are used (bhc/Spline.m:186-197, same 1e-6 rule)
+static std::vector<double> spline_table2(const double *k, int J)
+{
+    std::vector<double> t((size_t)J * kSpl2Stride);
+    for (int j = 0; j < J; ++j) {
+        const double a = k[j], b = k[j + 1], c = k[j + 2];
+        double *e = &t[(size_t)j * kSpl2Stride];
+        e[0] = -((a + b) * (a * a + b * b)) / 12 + ((b + c) * (b * b + c * c)) / 12;
+        e[1] = (pow(a, 4) + pow(a, 3) * b + a * a * b * b + a * pow(b, 3) + pow(b, 4)) / 20 -
+               (pow(b, 4) + pow(b, 3) * c + b * b * c * c + b * pow(c, 3) + pow(c, 4)) / 20;
+        e[2] = -((a + b) * (a * a + a * b + b * b) * (a * a - a * b + b * b)) / 60 +
+               ((b + c) * (b * b + b * c + c * c) * (b * b - b * c + c * c)) / 60;
+        e[3] = (pow(a, 6) + pow(a, 5) * b + pow(a, 4) * b * b + pow(a, 3) * pow(b, 3) + a * a * pow(b, 4) +
+                a * pow(b, 5) + pow(b, 6)) / 252 -
+               (pow(b, 6) + pow(b, 5) * c + pow(b, 4) * c * c + pow(b, 3) * pow(c, 3) + b * b * pow(c, 4) +
+                b * pow(c, 5) + pow(c, 6)) / 252;
+        e[4] = cbrt(fabs(1e-6 * e[0] / e[3]));
+    }
+    return t;
+}
+
+// Density Hessian weight per ray at the saved s: y = Ts (Phi v) in, h y out
+// (the backprojection input), per-block partials of sum h y^2.
+__global__ void __launch_bounds__(kTermThreads)
+k_bhc_hess(const float *__restrict__ s_saved, float *__restrict__ y, long long nrays, BhcArgs a,
+           const double *__restrict__ tab2_g)
+{
+    __shared__ double sm[kMaxJ * (kSplStride + kSpl2Stride + 1)];
+    __shared__ double red[kTermThreads / 32];
+    for (int i = threadIdx.x; i < a.J * kSplStride; i += blockDim.x) sm[i] = a.tab[i];
+    for (int i = threadIdx.x; i < a.J * kSpl2Stride; i += blockDim.x) sm[kMaxJ * kSplStride + i] = tab2_g[i];
+    for (int i = threadIdx.x; i < a.J; i += blockDim.x) sm[kMaxJ * (kSplStride + kSpl2Stride) + i] = a.Ie[i];
+    __syncthreads();
+    const double *tab = sm, *tab2 = sm + kMaxJ * kSplStride, *Ie = sm + kMaxJ * (kSplStride + kSpl2Stride);
+    double q = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
+         i += (long long)gridDim.x * blockDim.x) {
+        const SplineEval2 e = b1_eval2((double)s_saved[i], tab, tab2, Ie, a.J);
+        const double m = (double)a.imea[i];
+        const double h = ray_curvature(a.noise, e.BL, m) * e.sBL * e.sBL + ray_terms(a.noise, e.BL, m).r * e.ssBL;
+        const double yi = a.Ts * (double)y[i];
+        y[i] = (float)(h * yi);
+        q = fma(h * yi, yi, q);
+    }
+    q = block_sum_any(q, red);
+    if (threadIdx.x == 0) a.part[blockIdx.x] = q;
+}
+
 }  // namespace ctprj
 
 using namespace ctprj;
@@ -229,15 +278,19 @@ extern "C" int ctprj_bhc_create(ctprj_plan *plan, int J, const double *kappa_nod
     m->J = J;
     m->Ts = Ts;
     const std::vector<double> tab = spline_table(kappa_nodes, J);
+    const std::vector<double> tab2 = spline_table2(kappa_nodes, J);
     const size_t nr = (size_t)plan->g.np * plan->g.W;
     int st;
     if ((st = cuda_error(cudaMalloc((void **)&m->d_tab, sizeof(double) * tab.size()), "spline table")) ||
         (st = cuda_error(cudaMemcpy(m->d_tab, tab.data(), sizeof(double) * tab.size(),
                                     cudaMemcpyHostToDevice), "spline upload")) ||
+        (st = cuda_error(cudaMalloc((void **)&m->d_tab2, sizeof(double) * tab2.size()), "spline table")) ||
+        (st = cuda_error(cudaMemcpy(m->d_tab2, tab2.data(), sizeof(double) * tab2.size(),
+                                    cudaMemcpyHostToDevice), "spline upload")) ||
         (st = cuda_error(cudaMalloc((void **)&m->d_s, sizeof(float) * nr), "ray state")) ||
         (st = cuda_error(cudaMalloc((void **)&m->d_r, sizeof(float) * nr), "ray state")) ||
         (st = cuda_error(cudaMalloc((void **)&m->d_w, sizeof(float) * nr), "ray state"))) {
-        cudaFree(m->d_tab); cudaFree(m->d_s); cudaFree(m->d_r); cudaFree(m->d_w);
+        cudaFree(m->d_tab); cudaFree(m->d_tab2); cudaFree(m->d_s); cudaFree(m->d_r); cudaFree(m->d_w);
         delete m;
         return st;
     }
@@ -258,10 +311,12 @@ extern "C" void ctprj_bhc_destroy(ctprj_bhc *m)
     if (!m) return;
     PlanDevice pd(m->plan->device);
     cudaFree(m->d_tab);
+    cudaFree(m->d_tab2);
     cudaFree(m->d_s);
     cudaFree(m->d_r);
     cudaFree(m->d_w);
     cudaFree(m->d_part);
+    cudaFree(m->d_hsino);
     delete m;
 }
 
@@ -277,6 +332,7 @@ static BhcArgs bhc_args(ctprj_bhc *m, const double *d_Ie, const float *d_imea, i
     a.r_out = keep ? m->d_r : nullptr;
     a.w_out = keep ? m->d_w : nullptr;
     a.part = m->d_part;
+    a.noise = m->noise;
     return a;
 }
 
@@ -354,6 +410,40 @@ extern "C" int ctprj_bhc_basis(ctprj_bhc *m, const float *d_sino, double *d_A, v
     k_bhc_basis<<<4 * spectrum_blocks(), 256, 0, (cudaStream_t)stream>>>(d_sino, nr, m->d_tab, m->J,
                                                                          m->Ts, d_A);
     return cuda_error(cudaGetLastError(), "basis matrix");
+}
+
+extern "C" int ctprj_bhc_set_noise(ctprj_bhc *m, int noise)
+{
+    if (!m) return set_error(CTPRJ_EINVAL, "NULL model");
+    if (noise != CTPRJ_NOISE_POISSON && noise != CTPRJ_NOISE_GAUSSIAN)
+        return set_error(CTPRJ_EINVAL, "unknown noise model %d", noise);
+    m->noise = noise;
+    m->saved = 0;   // the saved weights belong to the other model
+    return CTPRJ_OK;
+}
+
+extern "C" int ctprj_bhc_hessian(ctprj_bhc *m, const double *d_Ie, const float *d_imea, const float *d_v,
+                                 float *d_Hv, double *d_vHv, void *stream)
+{
+    if (!m || !d_Ie || !d_imea || !d_v) return set_error(CTPRJ_EINVAL, "NULL argument");
+    if (!d_Hv && !d_vHv) return set_error(CTPRJ_EINVAL, "nothing requested");
+    if (!m->saved) return set_error(CTPRJ_EINVAL, "the Hessian needs a saved forward state");
+    PlanDevice pd(m->plan->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const long long nr = (long long)m->plan->g.np * m->plan->g.W;
+    int st;
+    if (!m->d_hsino &&
+        (st = cuda_error(cudaMalloc((void **)&m->d_hsino, sizeof(float) * nr), "Hessian scratch")))
+        return st;
+    const int blocks = 4 * spectrum_blocks();
+    if ((st = ensure_parts(m, blocks))) return st;
+    if ((st = ctprj_forward(m->plan, d_v, m->d_hsino, s))) return st;
+    k_bhc_hess<<<blocks, kTermThreads, 0, s>>>(m->d_s, m->d_hsino, nr, bhc_args(m, d_Ie, d_imea, 0),
+                                                m->d_tab2);
+    if (d_vHv) k_sum_columns<<<1, 32, 0, s>>>(m->d_part, blocks, 1, d_vHv);
+    if ((st = cuda_error(cudaGetLastError(), "Hessian weights"))) return st;
+    if (d_Hv) return launch_backward(m->plan, m->d_hsino, d_Hv, 0, nullptr, s, (float)m->Ts);
+    return CTPRJ_OK;
 }
 
 extern "C" int ctprj_bhc_state(ctprj_bhc *m, const float **d_s, const float **d_r, const float **d_w)

@@ -11,12 +11,14 @@
 //                 adjoint at xbar, a majorisation line search on the fused
 //                 forward, momentum restart (ctprj_bhc_reconstruct below);
 //  spectrum step  Newton on Ie >= 0: gradient A^T (1 - m/Ir) and Hessian
-//                 A^T diag(m / Ir^2) A reduced in FP64 from the rays x J basis
+//                 A^T diag(m / Ir^2) A (Gaussian model: A^T (Err / Ir) and the
+//                 Gauss-Newton A^T diag(1 / Ir^2) A) reduced in FP64 from the rays x J basis
 //                 matrix A of the current projections, the quadratic model
 //                 minimised over Ie >= 0 by an active-set method in one warp
 //                 (FP64 Cholesky, diagonal lifted until positive definite as
 //                 bhc/ActiveSet.m:62-76 lifts the eigenvalues), then a line
 //                 search shrinking the step by 0.8 (ActiveSet stepShrnk).
+#include <cfloat>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -35,7 +37,7 @@ constexpr int kMaxH = kMaxJ * (kMaxJ + 1) / 2;
 // Ie; layout part[block * (1 + J + J(J+1)/2)]
 __global__ void __launch_bounds__(kIeThreads)
 k_ie_eval(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
-          const double *__restrict__ Ie, int want_h, double *__restrict__ part)
+          const double *__restrict__ Ie, int want_h, int noise, double *__restrict__ part)
 {
     __shared__ double As[kIeChunk][kMaxJ];
     __shared__ double rs[kIeChunk], ds[kIeChunk], fs[kIeChunk];
@@ -66,9 +68,10 @@ k_ie_eval(const double *__restrict__ A, const float *__restrict__ m, long long n
             double Ir = 0.0;
             for (int j = 0; j < J; ++j) Ir = fma(As[threadIdx.x][j], Is[j], Ir);
             const double mi = (double)m[c0 + threadIdx.x];
-            rs[threadIdx.x] = 1.0 - mi / Ir;
-            ds[threadIdx.x] = mi / (Ir * Ir);
-            fs[threadIdx.x] = poisson_term(Ir, mi);
+            const RayTerms rt = ray_terms(noise, Ir, mi);
+            rs[threadIdx.x] = rt.r;
+            ds[threadIdx.x] = ray_curvature_model(noise, Ir, mi);
+            fs[threadIdx.x] = rt.f;
         }
         __syncthreads();
         if (threadIdx.x == 0)
@@ -102,6 +105,40 @@ __global__ void k_ie_sum(const double *__restrict__ part, int nblocks, int strid
     }
 }
 
+// Cholesky factorisation, by one warp, of the Jacobi-scaled block
+// H[F][F] / (dg_a dg_b) + lift I of the nf coefficients Fidx[0..nf) into L
+// (lane r owns row r).  Fails (warp-uniformly) when a pivot is not above
+// 1e-14 (1 + lift).
+__device__ bool warp_cholesky(double (*L)[kMaxJ + 1], const double (*H)[kMaxJ + 1], const int *Fidx,
+                              const double *dgs, int nf, double lift)
+{
+    const int r = threadIdx.x;
+    if (r < nf) {
+        const int jr = Fidx[r];
+        for (int b = 0; b <= r; ++b) {
+            const int jb = Fidx[b];
+            L[r][b] = H[jr][jb] / (dgs[jr] * dgs[jb]) + (b == r ? lift : 0.0);
+        }
+    }
+    bool ok = true;
+    for (int k = 0; k < nf; ++k) {
+        __syncwarp();
+        const double d = L[k][k];
+        if (!(d > 1e-14 * (1.0 + lift))) { ok = false; break; }
+        const double lk = sqrt(d);
+        __syncwarp();
+        if (r == k) L[k][k] = lk;
+        if (r > k && r < nf) L[r][k] /= lk;
+        __syncwarp();
+        if (r > k && r < nf) {
+            const double lrk = L[r][k];
+            for (int b = k + 1; b <= r; ++b) L[r][b] = fma(-lrk, L[b][k], L[r][b]);
+        }
+    }
+    __syncwarp();
+    return ok;
+}
+
 // The Newton direction of the spectrum step.  The quadratic model
 //   q(y) = 1/2 y'Hy + c'y,   c = g - H Ie,
 // is minimised over y >= 0 by a primal active-set method started at y = Ie
@@ -111,12 +148,15 @@ __global__ void k_ie_sum(const double *__restrict__ part, int nblocks, int strid
 // moves the active set one constraint at a time; here the subproblem is solved
 // to its optimum every Newton step, which is what makes the outer iteration
 // converge in a few steps although H spans many decades.
-// On each free set F, H_FF z_F = -c_F is solved by a Cholesky factorisation of
-// the Jacobi-scaled block (unit diagonal), the diagonal lifted until every
-// pivot stays above 1e-14 (bhc/ActiveSet.m:62-76 lifts the eigenvalues of the
-// reduced Hessian the same way).  A full step to z ends in a multiplier check
-// (release the most negative lambda_j = (Hy + c)_j of W); a blocked step adds
-// the blocking coefficient to W.
+// H is first made positive definite: its Jacobi-scaled form (unit diagonal) is
+// factored with the diagonal lifted (0, then 1e-14, x10) until every pivot
+// stays above 1e-14, and the lift is kept for the whole subproblem, so that the
+// model is convex (bhc/ActiveSet.m:62-76 lifts the eigenvalues of the reduced
+// Hessian the same way; the Gaussian model's Hessian can be indefinite).
+// On each free set F, H_FF z_F = -c_F is solved through the same scaled
+// factorisation.  A full step to z ends in a multiplier check (release the most
+// negative lambda_j = (Hy + c)_j of W); a blocked step adds the blocking
+// coefficient to W.
 // One warp: lane t owns coefficient t; inside a factorisation lane r owns row
 // r of the free block.  All branches that end loops are warp-uniform.
 __global__ void __launch_bounds__(32)
@@ -129,6 +169,7 @@ k_ie_qp(const double *__restrict__ fgh, const double *__restrict__ Ie, int J, do
     __shared__ int Fidx[kMaxJ];
     const unsigned full = 0xffffffffu;
     const int t = threadIdx.x;
+    const unsigned below = (1u << t) - 1u;
     const double *g = fgh + 1, *hp = fgh + 1 + J;
     if (t < J)
         for (int k = t; k < J; ++k) {
@@ -142,6 +183,26 @@ k_ie_qp(const double *__restrict__ fgh, const double *__restrict__ Ie, int J, do
     const bool fixed = !(t < J) || !(H[t < J ? t : 0][t < J ? t : 0] > 0.0);
     const double ie = t < J ? Ie[t] : 0.0;
     const double dg = fixed ? 1.0 : sqrt(H[t][t]);
+    dgs[t] = dg;
+    // convexify: the smallest lift of the scaled diagonal that factors
+    {
+        const unsigned am = __ballot_sync(full, !fixed);
+        if (!fixed) Fidx[__popc(am & below)] = t;
+        __syncwarp();
+        double lift = 0.0;
+        bool ok = false;
+        for (int attempt = 0; attempt < 40 && !ok; ++attempt) {
+            ok = warp_cholesky(L, H, Fidx, dgs, __popc(am), lift);
+            if (!ok) lift = lift == 0.0 ? 1e-14 : lift * 10.0;
+        }
+        if (!ok) {   // nothing sensible to do: no step
+            if (t < J) dir[t] = 0.0;
+            if (t == 0 && qp_iters) *qp_iters = -1;
+            return;
+        }
+        if (!fixed) H[t][t] *= 1.0 + lift;
+        __syncwarp();
+    }
     double c = 0.0;
     if (t < J) {
         double hy = 0.0;
@@ -151,68 +212,43 @@ k_ie_qp(const double *__restrict__ fgh, const double *__restrict__ Ie, int J, do
     double y = fixed ? ie : fmax(ie, 0.0);
     bool inW = !fixed && !(ie > 0.0);
     cs[t] = c;
-    dgs[t] = dg;
     int it = 0;
     for (; it < 8 * J + 16; ++it) {
         const bool fr = !fixed && !inW;
         const unsigned fm = __ballot_sync(full, fr);
         const int nf = __popc(fm);
-        if (fr) Fidx[__popc(fm & ((1u << t) - 1u))] = t;
+        if (fr) Fidx[__popc(fm & below)] = t;
         __syncwarp();
         double z = y;
-        bool solved = true;
         if (nf > 0) {
-            const int r = t;   // row owned in the factorisation
-            const int jr = r < nf ? Fidx[r] : 0;
+            // principal blocks of a positive definite matrix factor without a
+            // lift; the retries only guard against rounding
             double lift = 0.0;
             bool ok = false;
             for (int attempt = 0; attempt < 40 && !ok; ++attempt) {
-                if (r < nf)
-                    for (int b = 0; b <= r; ++b) {
-                        const int jb = Fidx[b];
-                        L[r][b] = H[jr][jb] / (dgs[jr] * dgs[jb]) + (b == r ? lift : 0.0);
-                    }
-                ok = true;
-                for (int k = 0; k < nf; ++k) {
-                    __syncwarp();
-                    const double d = L[k][k];
-                    if (!(d > 1e-14 * (1.0 + lift))) { ok = false; break; }
-                    const double lk = sqrt(d);
-                    __syncwarp();
-                    if (r == k) L[k][k] = lk;
-                    if (r > k && r < nf) L[r][k] /= lk;
-                    __syncwarp();
-                    if (r > k && r < nf) {
-                        const double lrk = L[r][k];
-                        for (int b = k + 1; b <= r; ++b) L[r][b] = fma(-lrk, L[b][k], L[r][b]);
-                    }
-                }
-                __syncwarp();
+                ok = warp_cholesky(L, H, Fidx, dgs, nf, lift);
                 if (!ok) lift = lift == 0.0 ? 1e-14 : lift * 10.0;
             }
-            if (!ok) {
-                solved = false;
-            } else {
-                if (r < nf) rhs[r] = -cs[jr] / dgs[jr];
-                for (int k = 0; k < nf; ++k) {   // L w = rhs
-                    __syncwarp();
-                    const double wk = rhs[k] / L[k][k];
-                    __syncwarp();
-                    if (r == k) rhs[k] = wk;
-                    if (r > k && r < nf) rhs[r] = fma(-L[r][k], wk, rhs[r]);
-                }
-                for (int k = nf - 1; k >= 0; --k) {   // L^T v = w
-                    __syncwarp();
-                    const double vk = rhs[k] / L[k][k];
-                    __syncwarp();
-                    if (r == k) rhs[k] = vk;
-                    if (r < k) rhs[r] = fma(-L[k][r], vk, rhs[r]);
-                }
+            if (!ok) break;
+            const int r = t;
+            if (r < nf) rhs[r] = -cs[Fidx[r]] / dgs[Fidx[r]];
+            for (int k = 0; k < nf; ++k) {   // L w = rhs
                 __syncwarp();
-                if (fr) z = rhs[__popc(fm & ((1u << t) - 1u))] / dg;
+                const double wk = rhs[k] / L[k][k];
+                __syncwarp();
+                if (r == k) rhs[k] = wk;
+                if (r > k && r < nf) rhs[r] = fma(-L[r][k], wk, rhs[r]);
             }
+            for (int k = nf - 1; k >= 0; --k) {   // L^T v = w
+                __syncwarp();
+                const double vk = rhs[k] / L[k][k];
+                __syncwarp();
+                if (r == k) rhs[k] = vk;
+                if (r < k) rhs[r] = fma(-L[k][r], vk, rhs[r]);
+            }
+            __syncwarp();
+            if (fr) z = rhs[__popc(fm & below)] / dg;
         }
-        if (!solved) break;
         const double p = fr ? z - y : 0.0;
         // ratio test: the first coefficient to reach 0 along p
         double rv = (fr && p < 0.0) ? -y / p : INFINITY;
@@ -330,6 +366,35 @@ k_npg_extrapolate(const float *__restrict__ x, const float *__restrict__ xprev, 
     }
 }
 
+// per-block partials of sum (a_i - b_i) c_i (b may be NULL), FP64
+__global__ void __launch_bounds__(256)
+k_vec_dot(const float *__restrict__ a, const float *__restrict__ b, const float *__restrict__ c, long long n,
+          double *__restrict__ part)
+{
+    __shared__ double red[8];
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        acc = fma((double)a[i] - (b ? (double)b[i] : 0.0), (double)c[i], acc);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// out = x + alpha g
+__global__ void __launch_bounds__(256)
+k_axpy(const float *__restrict__ x, const float *__restrict__ g, float alpha, long long n, float *__restrict__ out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = fmaf(alpha, g[i], x[i]);
+}
+
 // basis matrix from the saved per-ray projections s (already scaled by Ts)
 __global__ void __launch_bounds__(256)
 k_basis_from_s(const float *__restrict__ s, long long nrays, const double *__restrict__ tab_g, int J,
@@ -429,7 +494,7 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
     double fcur = 0.0;
     int done = 0;
     for (int it = 0; it < newton_steps && !st; ++it) {
-        k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, 1, ws.part);
+        k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, 1, m->noise, ws.part);
         k_ie_sum<<<1, 256, 0, s>>>(ws.part, ws.blocks, w, w, ws.fgh);
         k_ie_qp<<<1, 32, 0, s>>>(ws.fgh, d_Ie, J, ws.dir, ws.qp_iters);
         if ((st = cuda_error(cudaGetLastError(), "spectrum Newton"))) break;
@@ -438,7 +503,7 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
         bool accepted = false, converged = false;
         for (int ls = 0; ls < 40; ++ls, step *= 0.8) {
             k_ie_trial<<<1, 32, 0, s>>>(d_Ie, ws.dir, ws.fgh, J, step, ws.trial);
-            k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, 0, ws.part);
+            k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, 0, m->noise, ws.part);
             k_ie_sum<<<1, 32, 0, s>>>(ws.part, ws.blocks, w, 1, ws.f1);
             double fn = 0.0, gd = 0.0;
             if ((st = cuda_error(cudaMemcpyAsync(&fn, ws.f1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
@@ -503,10 +568,69 @@ struct LoopBufs {
     }
 };
 
+double reduce_fetch(const double *part, int nblocks, double *d_out, cudaStream_t s, int *st)
+{
+    k_ie_sum<<<1, 32, 0, s>>>(part, nblocks, 1, 1, d_out);
+    double v = 0.0;
+    if (!*st) *st = cuda_error(cudaGetLastError(), "reduction");
+    if (!*st) *st = fetch(&v, d_out, 1, s);
+    return v;
+}
+
+// The initial inverse step t of the density step, as the reference's
+// stepSizeInit (npg/Methods.m:98-124):
+//   hessian:  t = g'Hg / g'g at x (Hessian of the saved state at x);
+//   BB:       t = |(g(x) - g(x - delta)) . delta| / |delta|^2 with delta along g.
+// The reference's BB step, |delta| = 1e-5, is below the resolution of a
+// single-precision image; here |delta| = 1e-3 |x| (1e-3 for x = 0).
+// NaN becomes 1 and 0 becomes DBL_EPSILON, as there; a negative g'Hg (the
+// exact Hessian of either model is indefinite far from the data, where the
+// reference's NPG then stops with "a negative step size") is taken by its
+// magnitude.
+int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *d_imea, int mode,
+                         LoopBufs &b, int pgb, double *t_out, cudaStream_t s)
+{
+    const long long npx = (long long)m->plan->g.n * m->plan->g.n;
+    int st = 0;
+    if ((st = likelihood(m, d_x, d_Ie, d_imea, b.f, b.sino, s)) ||
+        (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.gx, nullptr, s)))
+        return st;
+    k_vec_dot<<<pgb, 256, 0, s>>>(b.gx, nullptr, b.gx, npx, b.part);
+    const double gg = reduce_fetch(b.part, pgb, b.sum, s, &st);
+    if (st) return st;
+    double t = NAN;
+    if (mode == CTPRJ_STEP_HESSIAN) {
+        if ((st = ctprj_bhc_hessian(m, d_Ie, d_imea, b.gx, nullptr, b.sum + 1, s))) return st;
+        double gHg = 0.0;
+        if ((st = fetch(&gHg, b.sum + 1, 1, s))) return st;
+        t = fabs(gHg) / gg;   // the exact Hessian can curve down along g far from the data
+    } else {
+        k_vec_dot<<<pgb, 256, 0, s>>>(d_x, nullptr, d_x, npx, b.part);
+        const double xx = reduce_fetch(b.part, pgb, b.sum, s, &st);
+        if (st) return st;
+        const double dn = xx > 0.0 ? 1e-3 * sqrt(xx) : 1e-3;
+        const double scale = dn / sqrt(gg);   // delta = scale * g
+        k_axpy<<<pgb, 256, 0, s>>>(d_x, b.gx, (float)(-scale), npx, b.xbar);
+        if ((st = cuda_error(cudaGetLastError(), "BB step")) ||
+            (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, b.sino, s)) ||
+            (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.xn, nullptr, s)))
+            return st;
+        k_vec_dot<<<pgb, 256, 0, s>>>(b.gx, b.xn, b.gx, npx, b.part);
+        const double dgd = reduce_fetch(b.part, pgb, b.sum, s, &st) * scale;
+        if (st) return st;
+        t = fabs(dgd) / (scale * scale * gg);
+    }
+    if (std::isnan(t)) t = 1.0;
+    if (t == 0.0) t = DBL_EPSILON;
+    *t_out = t;
+    return CTPRJ_OK;
+}
+
 }  // namespace
 
 // The density step follows the reference's NPG class (npg/NPG.m main, with
-// the proximal map reduced to the projection on x >= 0):
+// the proximal map reduced to the projection on x >= 0), or its PG class
+// (npg/PG.m: the same without extrapolation and restart):
 //   theta' = (1 + sqrt(1 + 4 theta^2)) / 2,  xbar = max(0, x + (theta-1)/theta' (x - xprev));
 //   f, grad at xbar;  candidate xn = max(0, xbar - grad / t), accepted when
 //   f(xn) <= f(xbar) + grad.(xn - xbar) + t/2 |xn - xbar|^2 (utils/Utils.m
@@ -515,9 +639,11 @@ struct LoopBufs {
 //   17 times); after 4 consecutive first-try successes t *= 0.5 once (failure
 //   of that try raises the count needed by 4);
 //   if f(xn) exceeds the cost of the previous iteration: restart without
-//   momentum (theta = 1) when xbar != x, else keep x (the reference's further
-//   retries with tighter inner ADMM tolerances do not apply to an exact
-//   projection).
+//   momentum (theta = 1) when xbar != x, else keep x when the majorisation
+//   failed or f(xbar) < f(xn) (PG: keep x when the majorisation failed or the
+//   cost rose).  The reference's further retries with tighter inner ADMM
+//   tolerances do not apply to an exact projection, and its reset of t to the
+//   Hessian estimate after a failed majorisation is not taken.
 // Then the spectrum step on the accepted density's projections, whose f
 // becomes the cost the next density step compares against
 // (bhc/beamhardenSpline.m:382-470).
@@ -550,6 +676,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         return st;
     }
     const int newton = opts->spectrum_newton_steps > 0 ? opts->spectrum_newton_steps : 2;
+    const bool pg = opts->density_method == CTPRJ_DENSITY_PG;
     double t = 1.0 / (opts->x_step > 0 ? opts->x_step : 1.0);   // inverse step size
     double theta = 0.0, cost = INFINITY;
     int p = 0, cumu = 0, cumu_tol = 4, evals = 0, restarts = 0, newton_done = 0;
@@ -563,6 +690,10 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     cudaEventCreate(&es1);
     st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "loop start");
     cudaEventRecord(e0, s);
+    if (!st && opts->init_step != CTPRJ_STEP_FIXED) {
+        st = initial_inverse_step(m, d_x, d_Ie, d_imea, opts->init_step, b, pgb, &t, s);
+        evals += opts->init_step == CTPRJ_STEP_BB ? 2 : 1;
+    }
     int done = 0;
     for (int it = 0; it < opts->iterations && !st; ++it) {
         double nc = 0.0;
@@ -570,7 +701,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         for (int pass = 0; pass < 3 && !st; ++pass) {
             ++p;
             const double theta1 = (1.0 + sqrt(1.0 + 4.0 * theta * theta)) / 2.0;
-            const float coef = (float)((theta - 1.0) / theta1);
+            const float coef = pg ? 0.0f : (float)((theta - 1.0) / theta1);
             k_npg_extrapolate<<<pgb, 256, 0, s>>>(d_x, b.xprev, npx, coef, b.xbar, b.part);
             k_ie_sum<<<1, 32, 0, s>>>(b.part, pgb, 2, 1, b.sum + 1);
             double f0 = 0.0, mom = 0.0;
@@ -619,17 +750,18 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                 }
             }
             if (st) break;
-            if (nc > cost) {
+            moved = true;
+            if (pg) {
+                if (!good_mm || nc > cost) moved = false;   // npg/PG.m: force convergence
+            } else if (nc > cost) {
                 if (good_mm && mom != 0.0 && pass < 2) {   // restart without momentum
                     theta = 1.0;
                     ++restarts;
                     continue;
                 }
-                nc = cost;   // keep x
-                moved = false;
-            } else {
-                moved = true;
+                if (!good_mm || f0 < nc) moved = false;     // npg/NPG.m: force convergence
             }
+            if (!moved) nc = cost;   // keep x
             theta = theta1;
             st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "accept");
             if (!st && moved)

@@ -60,8 +60,9 @@ struct BhcArgs {
     int J;
     double Ts;                // pixel size: s = Ts * (A x)
     const float *imea;        // measured intensity / I0 per ray (np * prjWidth)
-    float *s_out, *r_out, *w_out;   // per-ray s, 1 - m/BL, (1 - m/BL) dBL/ds; NULL: not kept
-    double *part;             // per-block partial sums of the Poisson terms
+    float *s_out, *r_out, *w_out;   // per-ray s, r = df/dBL, r dBL/ds; NULL: not kept
+    double *part;             // per-block partial sums of the likelihood terms
+    int noise;                // kNoisePoisson or kNoiseGaussian
 };
 
 enum { kModePlain = 0, kModeCount = 1, kModeBhc = 2 };
@@ -139,6 +140,9 @@ struct ctprj_bhc {
     double *d_part;           // per-block partials
     int part_cap;             // doubles in d_part
     int saved;                // the per-ray state holds the last forward's values
+    int noise;                // kNoisePoisson or kNoiseGaussian
+    double *d_tab2;           // second-derivative table, J * kSpl2Stride doubles
+    float *d_hsino;           // Hessian scratch, np * prjWidth floats (lazily)
 };
 
 namespace ctprj {

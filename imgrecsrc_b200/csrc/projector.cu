@@ -72,22 +72,23 @@ int launch_transpose(const float *src, float *dst, int n, cudaStream_t s)
 
 // ----------------------------------------------------------------- forward
 
-// Polychromatic epilogue of one sinogram entry (bhc/poissLAlpha.m:2-13 per
-// ray): s = Ts * proj, BL(s) and dBL/ds over the spectrum (FP64), and the
-// Poisson term; keeps s, 1 - m/BL and (1 - m/BL) dBL/ds when asked.
+// Polychromatic epilogue of one sinogram entry (bhc/poissLAlpha.m:2-13 and
+// bhc/gaussLAlpha.m:2-16 per ray): s = Ts * proj, BL(s) and dBL/ds over the
+// spectrum (FP64), and the likelihood term; keeps s, r = df/dBL and
+// r dBL/ds when asked.
 __device__ __forceinline__ double bhc_entry(const BhcArgs &a, const double *tab,
                                             const double *Ie, float proj, size_t idx)
 {
     const double s = a.Ts * (double)proj;
     const SplineEval e = b1_eval(s, tab, Ie, a.J);
     const double m = (double)__ldg(a.imea + idx);
-    const double r = 1.0 - m / e.BL;
+    const RayTerms t = ray_terms(a.noise, e.BL, m);
     if (a.w_out) {
-        a.w_out[idx] = (float)(r * e.sBL);
+        a.w_out[idx] = (float)(t.r * e.sBL);
         a.s_out[idx] = (float)s;
-        a.r_out[idx] = (float)r;
+        a.r_out[idx] = (float)t.r;
     }
-    return poisson_term(e.BL, m);
+    return t.f;
 }
 
 __device__ __forceinline__ double block_sum(double v, double *red)

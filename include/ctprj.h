@@ -123,7 +123,7 @@ int ctprj_count_updates(ctprj_plan *plan, long long *fwd, long long *bwd, void *
 
 /* ------------------------------------------------------------------------
  * Polychromatic beam-hardening model (bhc/Spline.m b1Iout, bhc/poissLAlpha.m,
- * bhc/poissLI.m) on a plan.  Per ray i: s_i = Ts (A x)_i, the degree-1
+ * bhc/poissLI.m; Gaussian variant below) on a plan.  Per ray i: s_i = Ts (A x)_i, the degree-1
  * B-spline spectrum model BL_i = sum_j Ie_j b_j(s_i) over J basis functions
  * on the J + 2 mass-attenuation nodes kappa (bhc/Spline.m:122-203), and the
  * Poisson negative log-likelihood of the measured intensity m_i (counts / I0):
@@ -164,9 +164,31 @@ int ctprj_bhc_terms(ctprj_bhc *model, const float *d_sino, const double *d_Ie,
  * solvers that work on the matrix. */
 int ctprj_bhc_basis(ctprj_bhc *model, const float *d_sino, double *d_A, void *stream);
 
-/* Device pointers of the saved per-ray state: s_i, 1 - m_i/BL_i and
- * (1 - m_i/BL_i) dBL/ds (np*prjWidth floats each). */
+/* Device pointers of the saved per-ray state: s_i, r_i = df/dBL_i
+ * (1 - m_i/BL_i for the Poisson model) and r_i dBL/ds (np*prjWidth floats
+ * each). */
 int ctprj_bhc_state(ctprj_bhc *model, const float **d_s, const float **d_r, const float **d_w);
+
+/* Noise model of the likelihood.  CTPRJ_NOISE_POISSON (the default):
+ * bhc/poissLAlpha.m, bhc/poissLI.m as above.  CTPRJ_NOISE_GAUSSIAN: the
+ * log-domain least squares of bhc/gaussLAlpha.m and bhc/gaussLI.m,
+ *   Err_i = log(BL_i / m_i),  f = sum_i Err_i^2 / 2,
+ *   df/dx = Ts A^T [Err/BL dBL/ds],  df/dIe_j = sum_i b_j(s_i) Err_i / BL_i,
+ * which needs m_i > 0.  Switching the model discards the saved state. */
+#define CTPRJ_NOISE_POISSON 0
+#define CTPRJ_NOISE_GAUSSIAN 1
+int ctprj_bhc_set_noise(ctprj_bhc *model, int noise);
+
+/* Density Hessian of f at the saved state (the `hessian` closures of
+ * bhc/poissLAlpha.m:15-28 and bhc/gaussLAlpha.m:18-31): with y = Ts A v and
+ * the per-ray weight h_i = q_i (dBL/ds)^2 + r_i d2BL/ds2 (q = d2f/dBL2:
+ * m/BL^2 Poisson, (1 - Err)/BL^2 Gaussian),
+ *   d_Hv  (n*n floats, may be NULL)       = Ts A^T (h y)     (opt = 1),
+ *   d_vHv (1 double on the device, NULL)  = sum_i h_i y_i^2  (opt = 2).
+ * d_Ie and d_imea must be those of the saved forward.  FP64 spline and
+ * reduction; one forward projection, plus one backprojection for d_Hv. */
+int ctprj_bhc_hessian(ctprj_bhc *model, const double *d_Ie, const float *d_imea, const float *d_v,
+                      float *d_Hv, double *d_vHv, void *stream);
 
 /* Static description of a status code, and the message of the last failure on
  * the calling thread. */

@@ -2,8 +2,9 @@
  * ctprj_bhc_loop.h -- the alternating beam-hardening reconstruction on the GPU.
  *
  * Counterpart of the reference's BHC driver loop (bhc/beamhardenSpline.m:
- * 340-570): one density step on the Poisson likelihood (the reference's NPG
- * class, npg/NPG.m, with the non-negativity projection as its proximal map),
+ * 340-570): one density step on the likelihood (the reference's NPG class,
+ * npg/NPG.m, or its PG class, npg/PG.m, with the non-negativity projection as
+ * the proximal map),
  * then a non-negative spectrum step, repeated.  Built on the model of
  * include/ctprj.h (ctprj_bhc_*): every likelihood and gradient of the density
  * step comes from the fused forward projection and its adjoint; the spectrum
@@ -23,6 +24,17 @@ extern "C" {
 
 #define CTPRJ_BHC_LOOP_MAX_TRACE 256
 
+/* initial density step (the reference's stepSizeInit, npg/Methods.m:98-124) */
+#define CTPRJ_STEP_FIXED 0    /* 1/t = x_step */
+#define CTPRJ_STEP_BB 1       /* finite-difference curvature along the gradient
+                                 (the reference's default, bhc/beamhardenSpline.m:73) */
+#define CTPRJ_STEP_HESSIAN 2  /* t = |g'Hg| / g'g from ctprj_bhc_hessian */
+
+/* density step method */
+#define CTPRJ_DENSITY_NPG 0   /* Nesterov proximal gradient with restart (npg/NPG.m,
+                                 the reference's default, bhc/beamhardenSpline.m:37) */
+#define CTPRJ_DENSITY_PG 1    /* proximal (projected) gradient (npg/PG.m) */
+
 typedef struct {
     int iterations;             /* alternating iterations */
     double x_step;              /* initial density step 1/t (<= 0: 1) */
@@ -31,6 +43,8 @@ typedef struct {
     int skip_spectrum;          /* 1: density steps only */
     int unfused;                /* 1: every likelihood from the plain forward projection
                                    plus a separate spectrum-terms kernel (comparison) */
+    int init_step;              /* CTPRJ_STEP_*: how the first 1/t is chosen */
+    int density_method;         /* CTPRJ_DENSITY_* */
 } ctprj_bhc_loop_opts;
 
 typedef struct {

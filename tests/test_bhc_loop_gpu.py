@@ -17,6 +17,12 @@ import imgrecsrc_b200 as ct  # noqa: E402
 from imgrecsrc_b200 import bhc, phantom  # noqa: E402
 
 
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 @pytest.fixture(scope="module", autouse=True)
 def _cuda():
     if not torch.cuda.is_available():
@@ -134,3 +140,35 @@ def test_fused_and_unfused_loops_agree():
     assert np.allclose(s1["cost"], s2["cost"], rtol=1e-12, atol=0)
     assert torch.equal(x1, x2)
     assert torch.allclose(I1, I2, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("method,noise", [("npg", "poisson"), ("pg", "poisson"), ("npg", "gaussian")])
+def test_loop_tracks_the_fp64_oracle_loop(method, noise):
+    """12 iterations of the GPU loop against the same algorithm in FP64
+    (oracle/bhc_loop_oracle.py over the FP64 projector): the line searches
+    take the same decisions, so the cost traces, the density and the spectrum
+    agree to the FP32 projections' accuracy."""
+    from oracle import bhc_loop_oracle as LO
+    g, Ts, x_true, k, I_true, m = setup_problem(J=20, seed=4)
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    model.set_noise(noise)
+    dx = torch.full((g.n, g.n), 1.0, device="cuda")
+    dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
+    dm = torch.from_numpy(m).cuda()
+    st = model.reconstruct(dx, dI, dm, iterations=12, x_step=1e-3, method=method)
+    fw = lambda x: oracle.forward(g, x)
+    bw = lambda y: oracle.backward(g, y.reshape(g.np, g.prjWidth))
+    xo, Io, so = LO.reconstruct(fw, bw, k, Ts, np.ones((g.n, g.n)), np.full(20, 1.0 / 20),
+                                m.astype(np.float64), 12, x_step=1e-3, method=method, noise=noise)
+    c, co = np.array(st["cost"]), np.array(so["cost"])
+    ex = rel(dx.cpu().numpy(), xo)
+    eI = rel(dI.cpu().numpy(), Io)
+    ec = float(np.max(np.abs(c - co) / np.abs(co)))
+    steps_equal = np.allclose(st["x_step"], so["x_step"], rtol=1e-12, atol=0)
+    print("loop vs FP64 oracle (%s, %s): max cost rel %.2e, x rel %.2e, Ie rel %.2e, same steps %s" % (
+        method, noise, ec, ex, eI, steps_equal))
+    assert steps_equal
+    assert ec < 1e-4
+    assert ex < 1e-4
+    assert eI < 1e-3
