@@ -105,6 +105,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(v, pg, device):
+    """The largest of the ranks' values of v (every rank gets it); v itself
+    when there is no process group."""
+    if pg is None:
+        return float(v)
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, updates_per_rank, t_max_ms):
+    """Whole-job throughput of `world` independent replicas in Gray-px/s: all
+    ranks' updates over the slowest rank's time."""
+    return world * updates_per_rank / (t_max_ms * 1e-3) / 1e9
+
+
 def init_dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -232,12 +249,8 @@ def our_arm(args):
     t_fwd = [ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)]
     t_bwd = [ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)]
     t_step = sum(a + b for a, b in zip(t_fwd, t_bwd)) / args.steps   # ms
-    t_max = t_step
-    if pg:
-        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t_max = float(tt.item())
-    value = world * (nnz_f + nnz_b) / (t_max * 1e-3) / 1e9
+    t_max = max_over_ranks(t_step, pg, "cuda")
+    value = replica_value(world, nnz_f + nnz_b, t_max)
 
     # roofline of the dominant kernel: 4 B per update + the compulsory image and
     # sinogram streams; duration from the CUDA events around its launch
@@ -249,7 +262,7 @@ def our_arm(args):
         kname, kms, kbytes = "k_transpose + k_forward<fan>", fwd_ms, 4 * nnz_f + compulsory + 8 * g.n * g.n
     peak, peak_kind = peaks()
     achieved = kbytes / (kms * 1e-3) / 1e9
-    traffic = PROFILED_TRAFFIC.get("k_backward" if bwd_ms >= fwd_ms else "k_forward")
+    traffic = profiled_traffic().get("k_backward_tiled<fan>" if bwd_ms >= fwd_ms else "k_forward<fan>")
 
     bhc_line = bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
     batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
@@ -275,12 +288,8 @@ def our_arm(args):
         ct.check(L.gpuPrj(ctypes.c_void_p(h_img.data_ptr()), ctypes.c_void_p(h_sino.data_ptr()), bytes([ct.FWD_BIT])))
         ct.check(L.gpuPrj(ctypes.c_void_p(h_back.data_ptr()), ctypes.c_void_p(h_sino.data_ptr()), bytes([ct.BWD_BIT])))
         e2e_times.append(time.perf_counter() - t0)
-    e2e_t = statistics.mean(e2e_times)
-    if pg:
-        tt = torch.tensor([e2e_t], device="cuda", dtype=torch.float64)
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        e2e_t = float(tt.item())
-    e2e_val = world * (nnz_f + nnz_b) / e2e_t / 1e9
+    e2e_t = max_over_ranks(statistics.mean(e2e_times), pg, "cuda")
+    e2e_val = replica_value(world, nnz_f + nnz_b, e2e_t * 1e3)
     img_b, sino_b = 4 * g.n * g.n, 4 * g.np * g.prjWidth
 
     line = {
@@ -494,7 +503,15 @@ def batch_leg(ct, flush, stream, steps):
 
 # dram__bytes_read.sum + dram__bytes_write.sum per launch from the ncu
 # captures summarised in profiles/ (None until captured)
-PROFILED_TRAFFIC = {}
+def profiled_traffic():
+    """DRAM bytes per launch of each profiled kernel from the committed ncu
+    summary (profiles/traffic.json), or {} when it is absent."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return {k: v["dram_bytes_per_launch"] for k, v in json.load(f)["kernels"].items()}
+    except (OSError, KeyError, ValueError):
+        return {}
 
 
 def main():
