@@ -115,7 +115,7 @@ static void free_plan(ctprj_plan *p)
     cudaFree(p->d_fview);
     cudaFree(p->d_bview);
     cudaFree(p->d_det);
-    cudaFree(p->d_imgT);
+    cudaFree(p->d_quad);
     cudaFree(p->d_count);
     cudaFree(p->d_ramp);
     cudaFree(p->d_fsino);
@@ -215,7 +215,7 @@ static int build_plan(const ctprj_geometry *geom, int device, ctprj_plan **out)
     if ((st = dg.status)) { delete p; return st; }
     if ((st = upload(&p->d_fview, fv)) || (st = upload(&p->d_bview, bv)) ||
         (st = upload(&p->d_det, de)) ||
-        (st = cuda_error(cudaMalloc((void **)&p->d_imgT, sizeof(float) * (size_t)g.n * g.n),
+        (st = cuda_error(cudaMalloc((void **)&p->d_quad, sizeof(float4) * quad_elems(g.n)),
                          "scratch allocation")) ||
         (st = cuda_error(cudaMalloc((void **)&p->d_count, sizeof(unsigned long long)),
                          "counter allocation"))) {
@@ -263,9 +263,9 @@ extern "C" int ctprj_forward(ctprj_plan *plan, const float *d_img, float *d_sino
     DeviceGuard dg(plan->device);
     if (dg.status) return dg.status;
     cudaStream_t s = (cudaStream_t)stream;
-    int st = launch_transpose(d_img, plan->d_imgT, plan->g.n, s);
+    int st = launch_quad(d_img, plan->d_quad, plan->g.n, s);
     if (st) return st;
-    return launch_forward(plan, d_img, plan->d_imgT, d_sino, nullptr, s);
+    return launch_forward(plan, plan->d_quad, d_sino, nullptr, s);
 }
 
 extern "C" int ctprj_backward(ctprj_plan *plan, const float *d_sino, float *d_img, void *stream)
@@ -288,7 +288,7 @@ extern "C" int ctprj_count_updates(ctprj_plan *plan, long long *fwd, long long *
         if ((st = cuda_error(cudaMemsetAsync(plan->d_count, 0, sizeof(unsigned long long), s),
                              "counter reset")))
             return st;
-        st = pass == 0 ? launch_forward(plan, nullptr, nullptr, nullptr, plan->d_count, s)
+        st = pass == 0 ? launch_forward(plan, nullptr, nullptr, plan->d_count, s)
                        : launch_backward(plan, nullptr, nullptr, 0, plan->d_count, s);
         if (st) return st;
         if ((st = cuda_error(cudaMemcpyAsync(&h[pass], plan->d_count, sizeof(unsigned long long),

@@ -104,8 +104,7 @@ int upload_lists(ctprj_batch *b)
     for (int i = 0; i < n; ++i) {
         fp[i + 1] = fp[i] + fwd_items(b->plans[of[i]], b->cfg.fwd_views);
         bp[i + 1] = bp[i] + bwd_items(b->plans[ob[i]]);
-        const int tn = (b->geoms[i].n + 31) / 32;
-        tp[i + 1] = tp[i] + (long long)tn * tn;
+        tp[i + 1] = tp[i] + quad_tiles(b->geoms[i].n);
     }
     b->ftotal = fp[n];
     b->btotal = bp[n];
@@ -159,7 +158,7 @@ int enqueue_forward(ctprj_batch *b, cudaStream_t s)
     if ((st = cuda_error(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), s), "batch counter")))
         return st;
     const BatchArgs a = fwd_args(b);
-    if ((st = launch_transpose_batch(a, s))) return st;
+    if ((st = launch_quad_batch(a, s))) return st;
     return launch_forward_batch(a, b->cfg.fwd_views, ctas(b, 0, b->cfg.fwd_views, b->cfg.fwd_occ), s);
 }
 
@@ -218,7 +217,7 @@ extern "C" int ctprj_batch_create(const ctprj_geometry *geoms, int nslices, int 
             memset(&h, 0, sizeof h);
             h.fp = make_fwd_params(b->plans[i]);
             h.bp = make_bwd_params(b->plans[i]);
-            h.imgT = b->plans[i]->d_imgT;
+            h.quad = b->plans[i]->d_quad;
             h.tiled = b->plans[i]->bwd_seg > 0;
             b->seg = std::max(b->seg, b->plans[i]->bwd_seg);
         }

@@ -149,11 +149,7 @@ k_bhc_basis(const float *__restrict__ sino, long long nrays, const double *__res
 __global__ void k_sum_columns(const double *__restrict__ part, int nrows, int ncols,
                               double *__restrict__ out)
 {
-    for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
-        double t = 0.0;
-        for (int b = 0; b < nrows; ++b) t += part[(size_t)b * ncols + c];
-        out[c] = t;
-    }
+    sum_partials(part, nrows, ncols, ncols, out);
 }
 
 static int spectrum_blocks()
@@ -344,12 +340,12 @@ extern "C" int ctprj_bhc_forward(ctprj_bhc *m, const float *d_x, const double *d
     cudaStream_t s = (cudaStream_t)stream;
     int st;
     if ((st = ensure_parts(m, forward_blocks(m->plan)))) return st;
-    if ((st = launch_transpose(d_x, m->plan->d_imgT, m->plan->g.n, s))) return st;
+    if ((st = launch_quad(d_x, m->plan->d_quad, m->plan->g.n, s))) return st;
     int nparts = 0;
-    if ((st = launch_forward_bhc(m->plan, d_x, m->plan->d_imgT, bhc_args(m, d_Ie, d_imea, save),
+    if ((st = launch_forward_bhc(m->plan, m->plan->d_quad, bhc_args(m, d_Ie, d_imea, save),
                                  &nparts, s)))
         return st;
-    k_sum_columns<<<1, 32, 0, s>>>(m->d_part, nparts, 1, d_f);
+    k_sum_columns<<<1, 256, 0, s>>>(m->d_part, nparts, 1, d_f);
     m->saved = save ? 1 : 0;
     return cuda_error(cudaGetLastError(), "likelihood reduction");
 }
@@ -365,7 +361,7 @@ extern "C" int ctprj_bhc_terms(ctprj_bhc *m, const float *d_sino, const double *
     int st;
     if ((st = ensure_parts(m, blocks))) return st;
     k_bhc_terms<<<blocks, kTermThreads, 0, s>>>(d_sino, nr, bhc_args(m, d_Ie, d_imea, save));
-    k_sum_columns<<<1, 32, 0, s>>>(m->d_part, blocks, 1, d_f);
+    k_sum_columns<<<1, 256, 0, s>>>(m->d_part, blocks, 1, d_f);
     m->saved = save ? 1 : 0;
     return cuda_error(cudaGetLastError(), "polychromatic terms");
 }
@@ -382,8 +378,8 @@ extern "C" int ctprj_bhc_backward(ctprj_bhc *m, const float *d_x, const double *
         if (!d_x || !d_Ie || !d_imea)
             return set_error(CTPRJ_EINVAL, "no saved forward state and no inputs to recompute it");
         if ((st = ensure_parts(m, forward_blocks(m->plan)))) return st;
-        if ((st = launch_transpose(d_x, m->plan->d_imgT, m->plan->g.n, s))) return st;
-        if ((st = launch_forward_bhc(m->plan, d_x, m->plan->d_imgT, bhc_args(m, d_Ie, d_imea, 1),
+        if ((st = launch_quad(d_x, m->plan->d_quad, m->plan->g.n, s))) return st;
+        if ((st = launch_forward_bhc(m->plan, m->plan->d_quad, bhc_args(m, d_Ie, d_imea, 1),
                                      nullptr, s)))
             return st;
     }
@@ -392,7 +388,7 @@ extern "C" int ctprj_bhc_backward(ctprj_bhc *m, const float *d_x, const double *
         if ((st = ensure_parts(m, blocks * m->J))) return st;
         const long long nr = (long long)m->plan->g.np * m->plan->g.W;
         k_bhc_spectrum<<<blocks, kSpecThreads, 0, s>>>(m->d_s, m->d_r, nr, m->d_tab, m->J, m->d_part);
-        k_sum_columns<<<1, 32, 0, s>>>(m->d_part, blocks, m->J, d_gIe);
+        k_sum_columns<<<1, 256, 0, s>>>(m->d_part, blocks, m->J, d_gIe);
         if ((st = cuda_error(cudaGetLastError(), "spectrum gradient"))) return st;
     }
     if (d_gx) {
@@ -440,7 +436,7 @@ extern "C" int ctprj_bhc_hessian(ctprj_bhc *m, const double *d_Ie, const float *
     if ((st = ctprj_forward(m->plan, d_v, m->d_hsino, s))) return st;
     k_bhc_hess<<<blocks, kTermThreads, 0, s>>>(m->d_s, m->d_hsino, nr, bhc_args(m, d_Ie, d_imea, 0),
                                                 m->d_tab2);
-    if (d_vHv) k_sum_columns<<<1, 32, 0, s>>>(m->d_part, blocks, 1, d_vHv);
+    if (d_vHv) k_sum_columns<<<1, 256, 0, s>>>(m->d_part, blocks, 1, d_vHv);
     if ((st = cuda_error(cudaGetLastError(), "Hessian weights"))) return st;
     if (d_Hv) return launch_backward(m->plan, m->d_hsino, d_Hv, 0, nullptr, s, (float)m->Ts);
     return CTPRJ_OK;

@@ -34,75 +34,103 @@ constexpr int kIeThreads = 256;
 constexpr int kMaxH = kMaxJ * (kMaxJ + 1) / 2;
 
 // per-block partials of f, g (J) and the upper triangle of H (J(J+1)/2) for
-// Ie; layout part[block * (1 + J + J(J+1)/2)]
-__global__ void __launch_bounds__(kIeThreads)
+// Ie; layout part[block * (1 + J + J(J+1)/2)].  Per chunk of kIeChunk rays the
+// block stages the basis rows A_i and the curvature-scaled rows sqrt(q_i) A_i
+// in shared memory; H = sum_i (sqrt(q_i) A_i)^T (sqrt(q_i) A_i) is then a small
+// GEMM in which thread (tj, tk) of a 16 x 16 grid accumulates the 2 x 2 tile
+// of rows 2tj.. and columns 2tk.. in registers (tiles below the diagonal
+// idle), g_j = sum_i A_ij r_i is split over the eight warps, and f over the
+// rays of the first two warps.  q >= 0 for both noise models' curvatures.
+__global__ void __launch_bounds__(kIeThreads, 2)
 k_ie_eval(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
           const double *__restrict__ Ie, int want_h, int noise, double *__restrict__ part)
 {
-    __shared__ double As[kIeChunk][kMaxJ];
-    __shared__ double rs[kIeChunk], ds[kIeChunk], fs[kIeChunk];
+    __shared__ __align__(16) double As[kIeChunk][kMaxJ];
+    __shared__ __align__(16) double Ss[kIeChunk][kMaxJ];
+    __shared__ double rs[kIeChunk], fs[kIeChunk];
     __shared__ double Is[kMaxJ];
-    const int nh = J * (J + 1) / 2;
-    for (int j = threadIdx.x; j < J; j += blockDim.x) Is[j] = Ie[j];
+    __shared__ double gpart[kIeThreads / 32][kMaxJ];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int j = t; j < kMaxJ; j += blockDim.x) Is[j] = j < J ? Ie[j] : 0.0;
+    const int tj = t >> 4, tk = t & 15;
+    const bool htile = want_h && 2 * tj <= 2 * tk + 1 && 2 * tj < J && 2 * tk < J;
+    double h00 = 0.0, h01 = 0.0, h10 = 0.0, h11 = 0.0;
     double f = 0.0, g = 0.0;
-    // entries of H owned by this thread: threadIdx.x + q * blockDim.x, q < 3
-    // (J(J+1)/2 <= 528 entries for J <= 32)
-    double h[3] = {0.0, 0.0, 0.0};
-    int hj[3] = {-1, -1, -1}, hk[3] = {-1, -1, -1};
-    for (int q = 0; q < 3; ++q) {
-        const int e = threadIdx.x + q * blockDim.x;
-        if (e >= nh) break;
-        int j = 0, rem = e;
-        while (rem >= J - j) { rem -= J - j; ++j; }
-        hj[q] = j;
-        hk[q] = j + rem;
-    }
     __syncthreads();
     for (long long c0 = (long long)blockIdx.x * kIeChunk; c0 < nrays; c0 += (long long)gridDim.x * kIeChunk) {
         const int nc = (int)(nrays - c0 < kIeChunk ? nrays - c0 : kIeChunk);
         __syncthreads();
-        for (int e = threadIdx.x; e < nc * J; e += blockDim.x)
-            As[e / J][e % J] = A[(size_t)(c0 + e / J) * J + e % J];
-        __syncthreads();
-        if (threadIdx.x < nc) {
-            double Ir = 0.0;
-            for (int j = 0; j < J; ++j) Ir = fma(As[threadIdx.x][j], Is[j], Ir);
-            const double mi = (double)m[c0 + threadIdx.x];
-            const RayTerms rt = ray_terms(noise, Ir, mi);
-            rs[threadIdx.x] = rt.r;
-            ds[threadIdx.x] = ray_curvature_model(noise, Ir, mi);
-            fs[threadIdx.x] = rt.f;
+        for (int e = t; e < kIeChunk * kMaxJ; e += blockDim.x) {
+            const int r = e / kMaxJ, j = e % kMaxJ;
+            As[r][j] = (r < nc && j < J) ? A[(size_t)(c0 + r) * J + j] : 0.0;
         }
         __syncthreads();
-        if (threadIdx.x == 0)
-            for (int i = 0; i < nc; ++i) f += fs[i];
-        if (threadIdx.x < J)
-            for (int i = 0; i < nc; ++i) g = fma(As[i][threadIdx.x], rs[i], g);
-        if (want_h) {
-#pragma unroll
-            for (int q = 0; q < 3; ++q)
-                if (hj[q] >= 0)
-                    for (int i = 0; i < nc; ++i) h[q] = fma(As[i][hj[q]] * As[i][hk[q]], ds[i], h[q]);
+        if (t < kIeChunk) {
+            double rr = 0.0, sq = 0.0, ff = 0.0;
+            if (t < nc) {
+                double Ir = 0.0;
+                for (int j = 0; j < J; ++j) Ir = fma(As[t][j], Is[j], Ir);
+                const double mi = (double)m[c0 + t];
+                const RayTerms rt = ray_terms(noise, Ir, mi);
+                rr = rt.r;
+                ff = rt.f;
+                sq = sqrt(ray_curvature_model(noise, Ir, mi));
+            }
+            rs[t] = rr;
+            fs[t] = ff;
+            if (want_h)
+                for (int j = 0; j < kMaxJ; ++j) Ss[t][j] = sq * As[t][j];
+        }
+        __syncthreads();
+        if (warp < 2) {   // f over the chunk, a fixed order
+            double v = fs[t];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) f += v;
+        }
+        if (lane < J)     // g: warp w takes rays w, w + 8, ...
+            for (int r = warp; r < nc; r += kIeThreads / 32) g = fma(As[r][lane], rs[r], g);
+        if (htile) {
+            for (int r = 0; r < nc; ++r) {
+                const double2 a = *reinterpret_cast<const double2 *>(&Ss[r][2 * tj]);
+                const double2 b = *reinterpret_cast<const double2 *>(&Ss[r][2 * tk]);
+                h00 = fma(a.x, b.x, h00);
+                h01 = fma(a.x, b.y, h01);
+                h10 = fma(a.y, b.x, h10);
+                h11 = fma(a.y, b.y, h11);
+            }
         }
     }
-    const int w = 1 + J + nh;
+    __syncthreads();
+    if (lane < kMaxJ) gpart[warp][lane] = g;
+    // f: lanes 0 of warps 0 and 1 hold the two halves
+    if (lane == 0 && warp < 2) rs[warp] = f;
+    __syncthreads();
+    const int w = 1 + J + J * (J + 1) / 2;
     double *out = part + (size_t)blockIdx.x * w;
-    if (threadIdx.x == 0) out[0] = f;
-    if (threadIdx.x < J) out[1 + threadIdx.x] = g;
-#pragma unroll
-    for (int q = 0; q < 3; ++q)
-        if (hj[q] >= 0) out[1 + J + threadIdx.x + q * blockDim.x] = want_h ? h[q] : 0.0;
+    if (t == 0) out[0] = rs[0] + rs[1];
+    if (t < J) {
+        double gs = 0.0;
+        for (int q = 0; q < kIeThreads / 32; ++q) gs += gpart[q][t];
+        out[1 + t] = gs;
+    }
+    if (htile) {
+        // entries (j, k), j <= k < J, of this thread's tile into the packed upper triangle
+        const int j0 = 2 * tj, k0 = 2 * tk;
+        double *h = out + 1 + J;
+        h[j0 * J - j0 * (j0 - 1) / 2 + (k0 - j0)] = h00;
+        if (k0 + 1 < J) h[j0 * J - j0 * (j0 - 1) / 2 + (k0 + 1 - j0)] = h01;
+        if (j0 + 1 < J && j0 + 1 <= k0) h[(j0 + 1) * J - (j0 + 1) * j0 / 2 + (k0 - j0 - 1)] = h10;
+        if (k0 + 1 < J) h[(j0 + 1) * J - (j0 + 1) * j0 / 2 + (k0 - j0)] = h11;
+    }
+    if (!want_h)
+        for (int e = t; e < J * (J + 1) / 2; e += blockDim.x) out[1 + J + e] = 0.0;
 }
 
 // out[c] = sum over blocks of part[b * stride + c] for c < ncols (fixed order, FP64)
 __global__ void k_ie_sum(const double *__restrict__ part, int nblocks, int stride, int ncols,
                          double *__restrict__ out)
 {
-    for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
-        double t = 0.0;
-        for (int b = 0; b < nblocks; ++b) t += part[(size_t)b * stride + c];
-        out[c] = t;
-    }
+    sum_partials(part, nblocks, stride, ncols, out);
 }
 
 // Cholesky factorisation, by one warp, of the Jacobi-scaled block
@@ -504,7 +532,7 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
         for (int ls = 0; ls < 40; ++ls, step *= 0.8) {
             k_ie_trial<<<1, 32, 0, s>>>(d_Ie, ws.dir, ws.fgh, J, step, ws.trial);
             k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, 0, m->noise, ws.part);
-            k_ie_sum<<<1, 32, 0, s>>>(ws.part, ws.blocks, w, 1, ws.f1);
+            k_ie_sum<<<1, 256, 0, s>>>(ws.part, ws.blocks, w, 1, ws.f1);
             double fn = 0.0, gd = 0.0;
             if ((st = cuda_error(cudaMemcpyAsync(&fn, ws.f1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
                 (st = fetch(&gd, ws.trial + J, 1, s)))
@@ -570,7 +598,7 @@ struct LoopBufs {
 
 double reduce_fetch(const double *part, int nblocks, double *d_out, cudaStream_t s, int *st)
 {
-    k_ie_sum<<<1, 32, 0, s>>>(part, nblocks, 1, 1, d_out);
+    k_ie_sum<<<1, 256, 0, s>>>(part, nblocks, 1, 1, d_out);
     double v = 0.0;
     if (!*st) *st = cuda_error(cudaGetLastError(), "reduction");
     if (!*st) *st = fetch(&v, d_out, 1, s);
@@ -703,7 +731,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             const double theta1 = (1.0 + sqrt(1.0 + 4.0 * theta * theta)) / 2.0;
             const float coef = pg ? 0.0f : (float)((theta - 1.0) / theta1);
             k_npg_extrapolate<<<pgb, 256, 0, s>>>(d_x, b.xprev, npx, coef, b.xbar, b.part);
-            k_ie_sum<<<1, 32, 0, s>>>(b.part, pgb, 2, 1, b.sum + 1);
+            k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 1, b.sum + 1);
             double f0 = 0.0, mom = 0.0;
             if ((st = cuda_error(cudaGetLastError(), "extrapolation")) ||
                 (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, b.sino, s)) ||
@@ -722,7 +750,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             while (true) {
                 ++ppp;
                 k_pg_step<<<pgb, 256, 0, s>>>(b.xbar, b.gx, npx, (float)(1.0 / t), b.xn, b.part);
-                k_ie_sum<<<1, 32, 0, s>>>(b.part, pgb, 2, 2, b.sum);
+                k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 2, b.sum);
                 double gd_dd[2];
                 if ((st = cuda_error(cudaGetLastError(), "density step")) ||
                     (st = likelihood(m, b.xn, d_Ie, d_imea, b.f + 1, b.sino, s)) ||

@@ -91,7 +91,7 @@ struct BatchSlice {
     FwdParams fp;
     BwdParams bp;
     const float *img;       // forward input
-    float *imgT;            // forward scratch (the slice plan's)
+    float4 *quad;           // forward scratch: the quad image (the slice plan's)
     float *sino;            // forward output
     const float *bsino;     // backward input
     float *bimg;            // backward output
@@ -123,7 +123,7 @@ struct ctprj_plan {
     ctprj::FwdView *d_fview;
     ctprj::BwdView *d_bview;
     ctprj::DetEntry *d_det;
-    float *d_imgT;            // scratch: transposed image (n*n)
+    float4 *d_quad;           // scratch: quad image, quad_elems(n) float4
     unsigned long long *d_count;
     // FBP: ramp-filter taps (2*prjWidth) and filtered-sinogram scratch
     float *d_ramp;
@@ -147,6 +147,36 @@ struct ctprj_bhc {
 
 namespace ctprj {
 
+// out[c] = sum over b < nrows of part[b * stride + c] for c < ncols, in FP64
+// and in an order fixed by the launch shape alone (results repeat bit for bit).
+// One block: with few columns each column is summed by the whole block (rows
+// strided over the threads, then a fixed tree), with many by one thread each.
+__device__ __forceinline__ void sum_partials(const double *__restrict__ part, int nrows, int stride,
+                                             int ncols, double *__restrict__ out)
+{
+    if (ncols >= (int)blockDim.x / 4) {
+        for (int c = threadIdx.x; c < ncols; c += blockDim.x) {
+            double t = 0.0;
+            for (int b = 0; b < nrows; ++b) t += part[(size_t)b * stride + c];
+            out[c] = t;
+        }
+        return;
+    }
+    __shared__ double red[1024];
+    for (int c = 0; c < ncols; ++c) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < nrows; b += blockDim.x) t += part[(size_t)b * stride + c];
+        red[threadIdx.x] = t;
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+            if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[c] = red[0];
+        __syncthreads();
+    }
+}
+
 // makes a plan's device current for the lifetime of the guard
 struct PlanDevice {
     int prev = -1;
@@ -166,19 +196,31 @@ int set_error(int status, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
 
 // launchers (projector.cu)
-int launch_transpose(const float *src, float *dst, int n, cudaStream_t s);
-int launch_forward(const ctprj_plan *p, const float *img, const float *imgT, float *sino,
+// the quad image of the forward pass (projector.cu): (half + 1) rows of
+// 2 half + 1 float4, built in 32 x 32 tiles
+__host__ __device__ inline size_t quad_elems(int n)
+{
+    const int half = (n - 1) / 2;
+    return (size_t)(half + 1) * (size_t)(2 * half + 1);
+}
+__host__ __device__ inline int quad_tiles(int n)
+{
+    const int half = (n - 1) / 2;
+    return ((2 * half + 1 + 31) / 32) * ((half + 1 + 31) / 32);
+}
+int launch_quad(const float *img, float4 *quad, int n, cudaStream_t s);
+int launch_forward(const ctprj_plan *p, const float4 *quad, float *sino,
                    unsigned long long *counter, cudaStream_t s);
 // fused forward projection + polychromatic epilogue; returns the number of
 // per-block partials written to a.part
-int launch_forward_bhc(const ctprj_plan *p, const float *img, const float *imgT,
+int launch_forward_bhc(const ctprj_plan *p, const float4 *quad,
                        const BhcArgs &a, int *nparts, cudaStream_t s);
 int forward_blocks(const ctprj_plan *p);
 int backward_max_span(const ctprj_plan *p, int *max_span);
 FwdParams make_fwd_params(const ctprj_plan *p);
 BwdParams make_bwd_params(const ctprj_plan *p);
 // persistent batch launches (projector.cu)
-int launch_transpose_batch(const BatchArgs &a, cudaStream_t s);
+int launch_quad_batch(const BatchArgs &a, cudaStream_t s);
 int launch_forward_batch(const BatchArgs &a, int views, int ctas, cudaStream_t s);
 int launch_backward_batch(const BatchArgs &a, int seg, int vb, int ctas, cudaStream_t s);
 int batch_max_ctas(int kind, int param, int *per_sm);

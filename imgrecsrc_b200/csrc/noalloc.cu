@@ -8,16 +8,17 @@
 // byte of the GPU.  ctprj_forward_noalloc serves them: the caller passes only
 // the geometry, the input image and the output sinogram, and the call uses
 // neither cudaMalloc nor cudaFree nor any allocating library routine.  The
-// scratch the forward pass needs -- the transposed image and the ray/view
-// tables -- lives in the file-scope arrays below, which every GPU that loads
-// this library holds until the process exits (about 4.4 MiB).
+// scratch the forward pass needs -- the quad image (the eight symmetric
+// copies of each pixel, twice the image's size) and the ray/view tables --
+// lives in the file-scope arrays below, which every GPU that loads this
+// library holds until the process exits (about 8.5 MiB).
 //
 // Limits: n <= 1024, prjWidth <= 4096, prjFull <= 8192 (so at most 1025 base
 // views).  Larger geometries are rejected with CTPRJ_ERANGE; they need the
 // plan API.
 //
 // All calls share these arrays.  Each call overwrites every element it later
-// reads (the transpose fills the whole n x n scratch and the tables are copied
+// reads (the quad image is rebuilt for the geometry and the tables are copied
 // in full for the geometry), so nothing has to start at zero, but calls whose
 // work overlaps on the GPU -- on different streams, or from different host
 // threads -- race on the shared arrays and must be serialised by the caller.
@@ -39,12 +40,13 @@ constexpr int kNoAllocMaxP = 8192;
 constexpr int kNoAllocMaxViews = kNoAllocMaxP / 8 + 1;
 constexpr int kNoAllocMaxDevices = 64;
 
-static __device__ __align__(256) float g_noalloc_imgT[kNoAllocMaxN * kNoAllocMaxN];
+// quad image of an n <= kNoAllocMaxN image: (half + 1) x (2 half + 1) float4
+static __device__ __align__(256) float4 g_noalloc_quad[(kNoAllocMaxN / 2 + 1) * (kNoAllocMaxN + 1)];
 static __device__ __align__(256) FwdView g_noalloc_view[kNoAllocMaxViews];
 static __device__ __align__(256) DetEntry g_noalloc_det[kNoAllocMaxW];
 
 struct NoAllocSymbols {
-    float *imgT;
+    float4 *quad;
     FwdView *view;
     DetEntry *det;
 };
@@ -67,7 +69,7 @@ static int noalloc_symbols(int dev, NoAllocSymbols *out)
     if (!g_noalloc_ready[dev]) {
         NoAllocSymbols s;
         int st;
-        if ((st = cuda_error(cudaGetSymbolAddress((void **)&s.imgT, g_noalloc_imgT),
+        if ((st = cuda_error(cudaGetSymbolAddress((void **)&s.quad, g_noalloc_quad),
                              "cudaGetSymbolAddress(scratch image)")) ||
             (st = cuda_error(cudaGetSymbolAddress((void **)&s.view, g_noalloc_view),
                              "cudaGetSymbolAddress(view table)")) ||
@@ -188,7 +190,7 @@ extern "C" int ctprj_forward_noalloc(const ctprj_geometry *geom, const float *d_
         return st;
     p.d_fview = sym.view;
     p.d_det = sym.det;
-    p.d_imgT = sym.imgT;
-    if ((st = launch_transpose(d_img, sym.imgT, g.n, s))) return st;
-    return launch_forward(&p, d_img, sym.imgT, d_sino, nullptr, s);
+    p.d_quad = sym.quad;
+    if ((st = launch_quad(d_img, sym.quad, g.n, s))) return st;
+    return launch_forward(&p, sym.quad, d_sino, nullptr, s);
 }

@@ -23,6 +23,7 @@
 // of O(n)); that keeps the projections within 1e-7..1e-6 of the FP64 oracle,
 // where the reference's own FP32 build is 1.5e-5 off on signed inputs.
 #include <cstdio>
+#include <type_traits>
 
 #include "ctprj_internal.h"
 #include "footprint.cuh"
@@ -39,35 +40,60 @@ namespace ctprj {
 #define CTPRJ_FWD_VIEWS 4
 #endif
 #ifndef CTPRJ_FWD_MINBLOCKS
-#define CTPRJ_FWD_MINBLOCKS 1
+#define CTPRJ_FWD_MINBLOCKS 6
 #endif
 constexpr int kFwdViews = CTPRJ_FWD_VIEWS;
 constexpr int kFwdThreads = 32 * kFwdViews;
 constexpr int kBwdTile = 16;   // 16 x 16 octant pixels per block
 
-// --------------------------------------------------------------- transpose
+// --------------------------------------------------------------- quad image
 
-__global__ void __launch_bounds__(256) k_transpose(const float *__restrict__ src,
-                                                   float *__restrict__ dst, int n)
+// The forward pass reads, for each pixel (x, y) a ray crosses, the eight images
+// of (x, y) under the symmetries of the square.  The quad image holds them as
+// two float4 per pixel: Q[yy][c] = {I(x, yy), I(x, -yy), I(yy, x), I(-yy, x)}
+// for rows yy = 0..half and columns c = x + half, x = -half..half, where
+// I(a, b) = img[(b + n/2) n + a + n/2]; (x, y) and (-x, y) give all eight.
+// One 32 x 32 tile of Q: the I(yy, x) and I(-yy, x) components are image
+// columns, staged through shared memory so that every global read is along a
+// row.
+__device__ __forceinline__ void quad_tile(const float *__restrict__ img, float4 *__restrict__ Q, int n,
+                                          int tile, float (&tz)[32][33], float (&tw)[32][33])
 {
-    __shared__ float tile[32][33];
-    const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int row = by + r, col = bx + threadIdx.x;
-        if (row < n && col < n) tile[r][threadIdx.x] = src[(size_t)row * n + col];
+    const int half = (n - 1) / 2, h2 = n / 2, QW = 2 * half + 1;
+    const int tcols = (QW + 31) / 32;
+    const int c0 = (tile % tcols) * 32, y0 = (tile / tcols) * 32;
+    __syncthreads();
+    // tz[i][j] = I(y0 + j, x_i), tw[i][j] = I(-(y0 + j), x_i) with x_i = c0 + i - half
+    for (int i = threadIdx.y; i < 32; i += 8) {
+        const int c = c0 + i, yy = y0 + threadIdx.x;
+        if (c < QW && yy <= half) {
+            const float *row = img + (size_t)(c - half + h2) * n + h2;
+            tz[i][threadIdx.x] = row[yy];
+            tw[i][threadIdx.x] = row[-yy];
+        }
     }
     __syncthreads();
-    for (int r = threadIdx.y; r < 32; r += 8) {
-        const int row = bx + r, col = by + threadIdx.x;
-        if (row < n && col < n) dst[(size_t)row * n + col] = tile[threadIdx.x][r];
+    for (int j = threadIdx.y; j < 32; j += 8) {
+        const int c = c0 + threadIdx.x, yy = y0 + j;
+        if (c < QW && yy <= half) {
+            const int x = c - half;
+            const float a = img[(size_t)(yy + h2) * n + x + h2];
+            const float b = img[(size_t)(h2 - yy) * n + x + h2];
+            Q[(size_t)yy * QW + c] = make_float4(a, b, tz[threadIdx.x][j], tw[threadIdx.x][j]);
+        }
     }
 }
 
-int launch_transpose(const float *src, float *dst, int n, cudaStream_t s)
+__global__ void __launch_bounds__(256) k_quad(const float *__restrict__ img, float4 *__restrict__ Q, int n)
 {
-    dim3 grid((n + 31) / 32, (n + 31) / 32), block(32, 8);
-    k_transpose<<<grid, block, 0, s>>>(src, dst, n);
-    return cuda_error(cudaGetLastError(), "transpose launch");
+    __shared__ float tz[32][33], tw[32][33];
+    quad_tile(img, Q, n, blockIdx.x, tz, tw);
+}
+
+int launch_quad(const float *img, float4 *Q, int n, cudaStream_t s)
+{
+    k_quad<<<quad_tiles(n), dim3(32, 8), 0, s>>>(img, Q, n);
+    return cuda_error(cudaGetLastError(), "quad image launch");
 }
 
 // ----------------------------------------------------------------- forward
@@ -109,8 +135,7 @@ __device__ __forceinline__ double block_sum(double v, double *red)
 // thread's Poisson terms in polychromatic mode.
 template <bool FAN, int MODE, int V>
 __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int by,
-                                               const float *__restrict__ img,
-                                               const float *__restrict__ imgT,
+                                               const float4 *__restrict__ quad,
                                                float *__restrict__ sino,
                                                unsigned long long *__restrict__ counter,
                                                const double *tab, const double *Ie)
@@ -168,21 +193,21 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
         const float dhb = FAN ? 0.5f * sTf * kbw : 0.0f;   // half beam width step per pixel
         const FootprintSat fp = make_footprint_sat(cRf, (float)sR);
 
-        const int N = g.n, half = g.half, h2 = g.h2;
+        const int half = g.half;
         float S[8];
 #pragma unroll
         for (int j = 0; j < 8; ++j) S[j] = 0.0f;
         unsigned long long nz = 0;
 
-        // rows y and -y of the image and of its transpose, centred on x = 0:
-        // a0[x] = I(x, y), a0[-x] = I(-x, y), a1[+-x] = I(+-x, -y),
-        // t0[x] = I(y, x), t0[-x] = I(y, -x), t1[+-x] = I(-y, +-x);
-        // stepped with the row
-        const float *a0 = img + (size_t)(half + h2) * N + h2;
-        const float *a1 = img + (size_t)(h2 - half) * N + h2;
-        const float *t0 = imgT + (size_t)(half + h2) * N + h2;
-        const float *t1 = imgT + (size_t)(h2 - half) * N + h2;
-        for (int y = half; y >= -half; --y, a0 -= N, a1 += N, t0 -= N, t1 += N) {
+        // The march down the rows.  Row y reads the quad row |y|:
+        // q[x] = {I(x, |y|), I(x, -|y|), I(|y|, x), I(-|y|, x)}, so that for
+        // y >= 0 the eight sums take, per pixel x,
+        //   S0 += I(x, y), S6 += I(-x, y), S4 += I(x, -y), S2 += I(-x, -y),
+        //   S5 += I(y, x), S3 += I(y, -x), S1 += I(-y, x), S7 += I(-y, -x)
+        // from q[x] and q[-x]; for y < 0 the pairs of components swap.
+        const int QW = 2 * half + 1;
+        auto march_row = [&](const int y, const float4 *__restrict__ q, auto neg) {
+            constexpr bool NEG = decltype(neg)::value;
             const float yf = (float)y;
             const float xl = fmaf(-yf, Slf, Alf), xr = fmaf(-yf, Srf, Arf);
             // nearest pixel to each edge; exact half-way ties (where the
@@ -192,7 +217,7 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
             int x1 = __float2int_rn(fminf(xr, (float)(half + 1)));
             x0 = max(x0, -half);
             x1 = min(x1, half);
-            if (x0 > x1) continue;
+            if (x0 > x1) return;
             // distance of pixel (x0, y) from the ray, in FP64 then rounded
             const float r0 = (float)fma((double)x0, cR, fma((double)y, sR, -off));
             const float hb0 = FAN ? 0.5f * fmaf(fmaf((float)x0, sTf, -yf * cTf), kbw, bwc)
@@ -206,15 +231,26 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
                     nz += (w != 0.0f);
                     continue;
                 }
-                S[0] = fmaf(w, __ldg(a0 + x), S[0]);
-                S[6] = fmaf(w, __ldg(a0 - x), S[6]);
-                S[4] = fmaf(w, __ldg(a1 + x), S[4]);
-                S[2] = fmaf(w, __ldg(a1 - x), S[2]);
-                S[5] = fmaf(w, __ldg(t0 + x), S[5]);
-                S[3] = fmaf(w, __ldg(t0 - x), S[3]);
-                S[1] = fmaf(w, __ldg(t1 + x), S[1]);
-                S[7] = fmaf(w, __ldg(t1 - x), S[7]);
+                const float4 pp = __ldg(q + x), pm = __ldg(q - x);
+                const float ap = NEG ? pp.y : pp.x, am = NEG ? pm.y : pm.x;   // I(+-x, y)
+                const float bp = NEG ? pp.x : pp.y, bm = NEG ? pm.x : pm.y;   // I(+-x, -y)
+                const float cp = NEG ? pp.w : pp.z, cm = NEG ? pm.w : pm.z;   // I(y, +-x)
+                const float dp = NEG ? pp.z : pp.w, dm = NEG ? pm.z : pm.w;   // I(-y, +-x)
+                S[0] = fmaf(w, ap, S[0]);
+                S[6] = fmaf(w, am, S[6]);
+                S[4] = fmaf(w, bp, S[4]);
+                S[2] = fmaf(w, bm, S[2]);
+                S[5] = fmaf(w, cp, S[5]);
+                S[3] = fmaf(w, cm, S[3]);
+                S[1] = fmaf(w, dp, S[1]);
+                S[7] = fmaf(w, dm, S[7]);
             }
+        };
+        {
+            const float4 *q = quad + (size_t)half * QW + half;   // row |y| = half, x = 0
+            for (int y = half; y >= 0; --y, q -= QW) march_row(y, q, std::false_type{});
+            q = quad + (size_t)QW + half;                          // row |y| = 1
+            for (int y = -1; y >= -half; --y, q += QW) march_row(y, q, std::true_type{});
         }
 
         // Scatter to the eight symmetric views (prj/cpuPrj.c:577-615); parallel
@@ -262,8 +298,8 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
 
 template <bool FAN, int MODE>
 __global__ void __launch_bounds__(kFwdThreads, CTPRJ_FWD_MINBLOCKS)
-k_forward(const FwdParams p, const float *__restrict__ img, const float *__restrict__ imgT,
-          float *__restrict__ sino, unsigned long long *__restrict__ counter)
+k_forward(const FwdParams p, const float4 *__restrict__ quad, float *__restrict__ sino,
+          unsigned long long *__restrict__ counter)
 {
     const double *tab = nullptr, *Ie = nullptr;
     if constexpr (MODE == kModeBhc) {
@@ -274,8 +310,8 @@ k_forward(const FwdParams p, const float *__restrict__ img, const float *__restr
         tab = sm;
         Ie = sm + kMaxJ * kSplStride;
     }
-    const double fsum = forward_rays<FAN, MODE, kFwdViews>(p, blockIdx.x, blockIdx.y, img, imgT,
-                                                           sino, counter, tab, Ie);
+    const double fsum = forward_rays<FAN, MODE, kFwdViews>(p, blockIdx.x, blockIdx.y, quad, sino,
+                                                           counter, tab, Ie);
     if constexpr (MODE == kModeBhc) {
         __shared__ double red[kFwdThreads / 32];
         const double t = block_sum(fsum, red);
@@ -308,30 +344,30 @@ int forward_blocks(const ctprj_plan *pl)
     return (int)(g.x * g.y);
 }
 
-int launch_forward(const ctprj_plan *pl, const float *img, const float *imgT, float *sino,
+int launch_forward(const ctprj_plan *pl, const float4 *quad, float *sino,
                    unsigned long long *counter, cudaStream_t s)
 {
     const FwdParams p = fwd_params(pl);
     const dim3 grid = fwd_grid(pl), block(kFwdThreads);
     const bool fan = pl->g.fan != 0;
     if (counter) {
-        if (fan) k_forward<true, kModeCount><<<grid, block, 0, s>>>(p, img, imgT, sino, counter);
-        else k_forward<false, kModeCount><<<grid, block, 0, s>>>(p, img, imgT, sino, counter);
+        if (fan) k_forward<true, kModeCount><<<grid, block, 0, s>>>(p, quad, sino, counter);
+        else k_forward<false, kModeCount><<<grid, block, 0, s>>>(p, quad, sino, counter);
     } else {
-        if (fan) k_forward<true, kModePlain><<<grid, block, 0, s>>>(p, img, imgT, sino, counter);
-        else k_forward<false, kModePlain><<<grid, block, 0, s>>>(p, img, imgT, sino, counter);
+        if (fan) k_forward<true, kModePlain><<<grid, block, 0, s>>>(p, quad, sino, counter);
+        else k_forward<false, kModePlain><<<grid, block, 0, s>>>(p, quad, sino, counter);
     }
     return cuda_error(cudaGetLastError(), "forward launch");
 }
 
-int launch_forward_bhc(const ctprj_plan *pl, const float *img, const float *imgT,
+int launch_forward_bhc(const ctprj_plan *pl, const float4 *quad,
                        const BhcArgs &a, int *nparts, cudaStream_t s)
 {
     FwdParams p = fwd_params(pl);
     p.bhc = a;
     const dim3 grid = fwd_grid(pl), block(kFwdThreads);
-    if (pl->g.fan) k_forward<true, kModeBhc><<<grid, block, 0, s>>>(p, img, imgT, nullptr, nullptr);
-    else k_forward<false, kModeBhc><<<grid, block, 0, s>>>(p, img, imgT, nullptr, nullptr);
+    if (pl->g.fan) k_forward<true, kModeBhc><<<grid, block, 0, s>>>(p, quad, nullptr, nullptr);
+    else k_forward<false, kModeBhc><<<grid, block, 0, s>>>(p, quad, nullptr, nullptr);
     if (nparts) *nparts = (int)(grid.x * grid.y);
     return cuda_error(cudaGetLastError(), "fused polychromatic forward launch");
 }
@@ -588,8 +624,10 @@ struct TiledSmem {
     float4 ra[VB][SEG];                      // D, cos B, sin B, half beam / qe
     float4 rb[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: hw, tb, hwr, iw
     float4 rc[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: c1, c2, i2b
-    float seg[VB][8][SEG];
-    float seg2[FAN ? 1 : VB][8][SEG];
+    // the eight (sixteen) mirrored samples of a staged ray, contiguous: two
+    // (four) 16-byte reads per detector and pixel
+    float4 seg[VB][SEG][2];
+    float4 seg2[FAN ? 1 : VB][FAN ? 1 : SEG][2];
     TileView tv[VB];
     FootprintSat pfs[VB];
 };
@@ -671,18 +709,30 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                 }
             }
         }
-        // B2: the mirrored sinogram samples, a warp per (view, image)
-        for (int pr = warp; pr < nb * 8; pr += kWarps) {
-            const int iv = pr >> 3, j = pr & 7;
+        // B2: the mirrored sinogram samples, a warp per view, a lane per
+        // detector (each load instruction reads one sinogram row contiguously)
+        for (int iv = warp; iv < nb; iv += kWarps) {
             const TileView &t = tv[iv];
             const BwdView &bv = p.view[i0 + iv];
-            const int row = bv.row[j];
-            const int row2 = FAN ? -1 : bv.row2[j];
             for (int kk = lane; kk < t.nseg; kk += 32) {
                 const int dt = t.klo + kk;
-                const int sg = j < 4 ? dt : -dt;
-                seg[iv][j][kk] = row >= 0 ? __ldg(sino + row + pC + sg) : 0.0f;
-                if (!FAN) seg2[FAN ? 0 : iv][j][kk] = row2 >= 0 ? __ldg(sino + row2 + pC - sg) : 0.0f;
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int row = bv.row[j];
+                    v[j] = row >= 0 ? __ldg(sino + row + pC + (j < 4 ? dt : -dt)) : 0.0f;
+                }
+                seg[iv][kk][0] = make_float4(v[0], v[1], v[2], v[3]);
+                seg[iv][kk][1] = make_float4(v[4], v[5], v[6], v[7]);
+                if (!FAN) {   // the point-reflected detectors of the opposite view
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+                        const int row2 = bv.row2[j];
+                        v[j] = row2 >= 0 ? __ldg(sino + row2 + pC - (j < 4 ? dt : -dt)) : 0.0f;
+                    }
+                    seg2[FAN ? 0 : iv][FAN ? 0 : kk][0] = make_float4(v[0], v[1], v[2], v[3]);
+                    seg2[FAN ? 0 : iv][FAN ? 0 : kk][1] = make_float4(v[4], v[5], v[6], v[7]);
+                }
             }
         }
         __syncthreads();
@@ -728,10 +778,26 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     } else {
                         w = footprint_weight_sat(a.x + du, hbpar, pfs[iv]);
                     }
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        S[j] = fmaf(w, seg[iv][j][kk], S[j]);
-                        if (!FAN) S[j] = fmaf(w, seg2[FAN ? 0 : iv][j][kk], S[j]);
+                    const float4 p0 = seg[iv][kk][0], p1 = seg[iv][kk][1];
+                    S[0] = fmaf(w, p0.x, S[0]);
+                    S[1] = fmaf(w, p0.y, S[1]);
+                    S[2] = fmaf(w, p0.z, S[2]);
+                    S[3] = fmaf(w, p0.w, S[3]);
+                    S[4] = fmaf(w, p1.x, S[4]);
+                    S[5] = fmaf(w, p1.y, S[5]);
+                    S[6] = fmaf(w, p1.z, S[6]);
+                    S[7] = fmaf(w, p1.w, S[7]);
+                    if (!FAN) {
+                        const float4 q0 = seg2[FAN ? 0 : iv][FAN ? 0 : kk][0];
+                        const float4 q1 = seg2[FAN ? 0 : iv][FAN ? 0 : kk][1];
+                        S[0] = fmaf(w, q0.x, S[0]);
+                        S[1] = fmaf(w, q0.y, S[1]);
+                        S[2] = fmaf(w, q0.z, S[2]);
+                        S[3] = fmaf(w, q0.w, S[3]);
+                        S[4] = fmaf(w, q1.x, S[4]);
+                        S[5] = fmaf(w, q1.y, S[5]);
+                        S[6] = fmaf(w, q1.z, S[6]);
+                        S[7] = fmaf(w, q1.w, S[7]);
                     }
                 }
             }
@@ -849,25 +915,13 @@ __device__ __forceinline__ long long next_item(unsigned long long *counter, long
     return *slot;
 }
 
-__global__ void __launch_bounds__(256) k_transpose_batch(const BatchArgs a)
+__global__ void __launch_bounds__(256) k_quad_batch(const BatchArgs a)
 {
-    __shared__ float tile[32][33];
+    __shared__ float tz[32][33], tw[32][33];
     for (long long e = blockIdx.x; e < a.ttotal; e += gridDim.x) {
         const int i = find_slot(a.tprefix, a.nslices, e);
         const BatchSlice &sl = a.slices[i];
-        const int n = sl.fp.g.n, tn = (n + 31) / 32;
-        const int local = (int)(e - a.tprefix[i]);
-        const int bx = (local % tn) * 32, by = (local / tn) * 32;
-        __syncthreads();
-        for (int r = threadIdx.y; r < 32; r += 8) {
-            const int row = by + r, col = bx + threadIdx.x;
-            if (row < n && col < n) tile[r][threadIdx.x] = sl.img[(size_t)row * n + col];
-        }
-        __syncthreads();
-        for (int r = threadIdx.y; r < 32; r += 8) {
-            const int row = bx + r, col = by + threadIdx.x;
-            if (row < n && col < n) sl.imgT[(size_t)row * n + col] = tile[threadIdx.x][r];
-        }
+        quad_tile(sl.img, sl.quad, sl.fp.g.n, (int)(e - a.tprefix[i]), tz, tw);
     }
 }
 
@@ -884,11 +938,9 @@ __global__ void __launch_bounds__(32 * V, 24 / V) k_forward_batch(const BatchArg
         const int gx = (sl.fp.nb + V - 1) / V;
         const int bx = local % gx, by = local / gx;
         if (sl.fp.g.fan)
-            forward_rays<true, kModePlain, V>(sl.fp, bx, by, sl.img, sl.imgT, sl.sino, nullptr,
-                                              nullptr, nullptr);
+            forward_rays<true, kModePlain, V>(sl.fp, bx, by, sl.quad, sl.sino, nullptr, nullptr, nullptr);
         else
-            forward_rays<false, kModePlain, V>(sl.fp, bx, by, sl.img, sl.imgT, sl.sino, nullptr,
-                                               nullptr, nullptr);
+            forward_rays<false, kModePlain, V>(sl.fp, bx, by, sl.quad, sl.sino, nullptr, nullptr, nullptr);
     }
 }
 
@@ -1005,11 +1057,11 @@ int launch_backward_stream(const BatchArgs &a, int seg, int vb, int ctas, const 
     return cuda_error(cudaGetLastError(), "streaming backward launch");
 }
 
-int launch_transpose_batch(const BatchArgs &a, cudaStream_t s)
+int launch_quad_batch(const BatchArgs &a, cudaStream_t s)
 {
     const long long blocks = a.ttotal < 65536 ? a.ttotal : 65536;
-    k_transpose_batch<<<(int)(blocks > 0 ? blocks : 1), dim3(32, 8), 0, s>>>(a);
-    return cuda_error(cudaGetLastError(), "batched transpose launch");
+    k_quad_batch<<<(int)(blocks > 0 ? blocks : 1), dim3(32, 8), 0, s>>>(a);
+    return cuda_error(cudaGetLastError(), "batched quad image launch");
 }
 
 int launch_forward_batch(const BatchArgs &a, int views, int ctas, cudaStream_t s)
