@@ -49,53 +49,51 @@ __device__ __forceinline__ float footprint_weight(float dist, float bw, const Fo
     return f.h * (trap_cdf(hb - dist, f) - trap_cdf(-hb - dist, f));
 }
 
-// The same weight with every clamp done by the FMA pipe's saturation to [0, 1]
-// instead of min/max on the ALU pipe.  With P = sat((u + b2)/w),
-// R = sat((u - b1)/w) and Q = sat((u + b1)/(2 b1)) the cumulative area is
-//   G(u) = w/2 (P^2 - R^2) + 2 b1 Q + w R,
-// and the coefficients below fold in the plateau height.  A ramp width or
-// shoulder width of zero gets a huge finite reciprocal whose saturated terms
-// are multiplied by that zero width, so axis-aligned and diagonal rays need no
-// branch.  The rounding of (u + b2)/w is bounded by b2 ulp(1) / w and is scaled
-// back by w, so the absolute error stays below ~1e-7 for any ramp width.
-struct FootprintSat {
+// The same weight without branches or min/max, every clamp done by the
+// arithmetic pipes' saturation to [0, 1].  In units of the ramp width w, with
+// v = u / w, the cumulative area of the trapezoid (plateau height h) is
+//   G(u) = h w/2 (P^2 - R'^2) + h 2 b1 Q + h w/2,
+//   P = sat(b2/w + v),  R' = sat(b2/w - v),  Q = sat(1/2 + v w/(2 b1))
+// (P: the rising ramp, R' = 1 - the falling ramp, Q: the plateau), and the
+// constant cancels in the difference of the two beam edges.  Callers pass the
+// distance and the half beam width already multiplied by 1/w (folded into
+// their per-ray coefficients), so a weight costs 14 arithmetic instructions.
+// A ramp width or shoulder width of zero (axis-aligned or diagonal rays) gets
+// a tiny floor: the huge ratios saturate and are multiplied by the zero width,
+// so no branch is needed.  The rounding of b2/w +- v is bounded by
+// b2 ulp(1) / w and is scaled back by h w/2: the absolute error stays below
+// ~1e-7 for any ramp width.
+struct FootprintV {
     float hw;    // h w / 2
     float tb;    // h 2 b1
-    float hwr;   // h w
-    float iw;    // 1 / w
     float c1;    // b2 / w
-    float c2;    // -b1 / w
-    float i2b;   // 1 / (2 b1)
+    float rho;   // w / (2 b1)
+    float iw;    // 1 / w: the caller's scale of distances and beam widths
 };
 
-__host__ __device__ __forceinline__ FootprintSat make_footprint_sat(float c, float s)
+__host__ __device__ __forceinline__ FootprintV make_footprint_v(float c, float s)
 {
     const Footprint f = make_footprint(c, s);
-    FootprintSat q;
+    FootprintV q;
     const float w = f.w > 1e-30f ? f.w : 1e-30f;
     const float tb = 2.0f * f.b1 > 1e-30f ? 2.0f * f.b1 : 1e-30f;
     q.iw = 1.0f / w;
     q.c1 = f.b2 * q.iw;
-    q.c2 = -f.b1 * q.iw;
-    q.i2b = 1.0f / tb;
+    q.rho = w / tb;
     q.hw = f.h * 0.5f * f.w;
     q.tb = f.h * 2.0f * f.b1;
-    q.hwr = f.h * f.w;
     return q;
 }
 
-__device__ __forceinline__ float trap_cdf_sat(float u, const FootprintSat &q)
+// weight for distance D = dist / w and half beam width H = hb / w
+__device__ __forceinline__ float footprint_weight_v(float D, float H, const FootprintV &q)
 {
-    const float P = __saturatef(fmaf(u, q.iw, q.c1));
-    const float R = __saturatef(fmaf(u, q.iw, q.c2));
-    const float Q = __saturatef(fmaf(u, q.i2b, 0.5f));
-    return fmaf(q.hw, fmaf(P, P, -R * R), fmaf(q.tb, Q, q.hwr * R));
-}
-
-// footprint weight for a beam of half-width hb
-__device__ __forceinline__ float footprint_weight_sat(float dist, float hb, const FootprintSat &q)
-{
-    return trap_cdf_sat(hb - dist, q) - trap_cdf_sat(-hb - dist, q);
+    const float v1 = H - D, v2 = -H - D;
+    const float P1 = __saturatef(q.c1 + v1), R1 = __saturatef(q.c1 - v1);
+    const float P2 = __saturatef(q.c1 + v2), R2 = __saturatef(q.c1 - v2);
+    const float Q1 = __saturatef(fmaf(v1, q.rho, 0.5f)), Q2 = __saturatef(fmaf(v2, q.rho, 0.5f));
+    const float X1 = fmaf(P1, P1, -R1 * R1), X2 = fmaf(P2, P2, -R2 * R2);
+    return fmaf(q.hw, X1 - X2, q.tb * (Q1 - Q2));
 }
 
 }  // namespace ctprj

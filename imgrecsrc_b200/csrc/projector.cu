@@ -35,12 +35,16 @@ namespace ctprj {
 // per warp: the warps march over nearly the same image lines at the same time,
 // so the rows they gather are shared in L1.  CTPRJ_FWD_VIEWS and
 // CTPRJ_FWD_MINBLOCKS (resident blocks asked of the register allocator) are
-// build-time launch-shape choices.
+// build-time launch-shape choices, as is CTPRJ_BWD_MINBLOCKS for the staged
+// backprojection.
 #ifndef CTPRJ_FWD_VIEWS
 #define CTPRJ_FWD_VIEWS 4
 #endif
 #ifndef CTPRJ_FWD_MINBLOCKS
-#define CTPRJ_FWD_MINBLOCKS 6
+#define CTPRJ_FWD_MINBLOCKS 7
+#endif
+#ifndef CTPRJ_BWD_MINBLOCKS
+#define CTPRJ_BWD_MINBLOCKS 5
 #endif
 constexpr int kFwdViews = CTPRJ_FWD_VIEWS;
 constexpr int kFwdThreads = 32 * kFwdViews;
@@ -191,7 +195,8 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
         const float Alf = (float)Al, Slf = (float)Sl, Arf = (float)Ar, Srf = (float)Sr;
         const float cRf = (float)cR, cTf = (float)cT, sTf = (float)sT;
         const float dhb = FAN ? 0.5f * sTf * kbw : 0.0f;   // half beam width step per pixel
-        const FootprintSat fp = make_footprint_sat(cRf, (float)sR);
+        const FootprintV fp = make_footprint_v(cRf, (float)sR);
+        const float cRw = cRf * fp.iw, dhbw = dhb * fp.iw;   // per-pixel steps in ramp units
 
         const int half = g.half;
         float S[8];
@@ -218,15 +223,16 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
             x0 = max(x0, -half);
             x1 = min(x1, half);
             if (x0 > x1) return;
-            // distance of pixel (x0, y) from the ray, in FP64 then rounded
-            const float r0 = (float)fma((double)x0, cR, fma((double)y, sR, -off));
-            const float hb0 = FAN ? 0.5f * fmaf(fmaf((float)x0, sTf, -yf * cTf), kbw, bwc)
-                                  : 0.5f * g.beamWidthF;
+            // distance of pixel (x0, y) from the ray, in FP64 then rounded;
+            // distances and half beam widths in units of the footprint's ramp
+            const float r0 = (float)fma((double)x0, cR, fma((double)y, sR, -off)) * fp.iw;
+            const float hb0 = (FAN ? 0.5f * fmaf(fmaf((float)x0, sTf, -yf * cTf), kbw, bwc)
+                                   : 0.5f * g.beamWidthF) * fp.iw;
             for (int x = x0; x <= x1; ++x) {
                 const float jf = (float)(x - x0);
-                const float dist = fmaf(jf, cRf, r0);
-                const float hb = FAN ? fmaf(jf, dhb, hb0) : hb0;
-                const float w = footprint_weight_sat(dist, hb, fp);
+                const float D = fmaf(jf, cRw, r0);
+                const float H = FAN ? fmaf(jf, dhbw, hb0) : hb0;
+                const float w = footprint_weight_v(D, H, fp);
                 if (MODE == kModeCount) {
                     nz += (w != 0.0f);
                     continue;
@@ -621,15 +627,14 @@ struct TileView {
 // shared memory of one staged tile
 template <bool FAN, int SEG, int VB>
 struct TiledSmem {
-    float4 ra[VB][SEG];                      // D, cos B, sin B, half beam / qe
-    float4 rb[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: hw, tb, hwr, iw
-    float4 rc[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: c1, c2, i2b
+    float4 ra[VB][SEG];                      // D, cos B, sin B, half beam / qe; all / w
+    float4 rb[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: hw, tb, c1, rho
     // the eight (sixteen) mirrored samples of a staged ray, contiguous: two
     // (four) 16-byte reads per detector and pixel
     float4 seg[VB][SEG][2];
     float4 seg2[FAN ? 1 : VB][FAN ? 1 : SEG][2];
     TileView tv[VB];
-    FootprintSat pfs[VB];
+    FootprintV pfs[VB];
 };
 
 // One tile of the staged backprojection (all threads of the block take part).
@@ -642,7 +647,6 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     const Geo &g = p.g;
     auto &ra = sm.ra;
     auto &rb = sm.rb;
-    auto &rc = sm.rc;
     auto &seg = sm.seg;
     auto &seg2 = sm.seg2;
     auto &tv = sm.tv;
@@ -688,7 +692,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
             t.klo = sp.klo;
             t.nseg = min(sp.nseg, SEG);   // the plan chose SEG above every span
             tv[iv] = t;
-            if (!FAN) pfs[iv] = make_footprint_sat(bv.cf, bv.sf);
+            if (!FAN) pfs[iv] = make_footprint_v(bv.cf, bv.sf);
         }
         __syncthreads();
         // B1: ray coefficients of the staged detectors, a warp per view
@@ -700,12 +704,12 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     const double D = fma(de.cB, t.uc - de.t, de.sB * t.vc);
                     const float cR = fmaf(de.cBf, t.cT, -de.sBf * t.sT);
                     const float sR = fmaf(de.sBf, t.cT, de.cBf * t.sT);
-                    const FootprintSat f = make_footprint_sat(cR, sR);
-                    ra[iv][kk] = make_float4((float)D, de.cBf, de.sBf, 0.5f * g.beamWidthF * de.invbq);
-                    rb[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.hw, f.tb, f.hwr, f.iw);
-                    rc[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.c1, f.c2, f.i2b, 0.0f);
+                    const FootprintV f = make_footprint_v(cR, sR);
+                    ra[iv][kk] = make_float4((float)D * f.iw, de.cBf * f.iw, de.sBf * f.iw,
+                                             0.5f * g.beamWidthF * de.invbq * f.iw);
+                    rb[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.hw, f.tb, f.c1, f.rho);
                 } else {
-                    ra[iv][kk] = make_float4((float)(t.uc - de.t), 0.0f, 0.0f, 0.0f);
+                    ra[iv][kk] = make_float4((float)(t.uc - de.t) * pfs[iv].iw, 0.0f, 0.0f, 0.0f);
                 }
             }
         }
@@ -766,17 +770,19 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                 dl = max(max(dl, -dmax) - t.klo, 0);
                 dr = min(min(dr, dmax) - t.klo, t.nseg - 1);
                 const float fbpw = FBP ? __fdividef(dF, qe) * __fdividef(dF, qe) : 1.0f;
+                const FootprintV fpar = FAN ? FootprintV{} : pfs[iv];
+                const float duw = FAN ? 0.0f : du * fpar.iw, Hpar = FAN ? 0.0f : hbpar * fpar.iw;
                 for (int kk = dl; kk <= dr; ++kk) {
                     const float4 a = ra[iv][kk];
                     float w;
                     if (FAN) {
-                        const float dist = fmaf(a.y, du, fmaf(a.z, dv, a.x));
-                        const float4 b = rb[FAN ? iv : 0][FAN ? kk : 0], c = rc[FAN ? iv : 0][FAN ? kk : 0];
-                        const FootprintSat f = {b.x, b.y, b.z, b.w, c.x, c.y, c.z};
-                        w = footprint_weight_sat(dist, qe * a.w, f);
+                        const float D = fmaf(a.y, du, fmaf(a.z, dv, a.x));
+                        const float4 b = rb[FAN ? iv : 0][FAN ? kk : 0];
+                        const FootprintV f = {b.x, b.y, b.z, b.w, 0.0f};
+                        w = footprint_weight_v(D, qe * a.w, f);
                         if (FBP) w *= fbpw;
                     } else {
-                        w = footprint_weight_sat(a.x + du, hbpar, pfs[iv]);
+                        w = footprint_weight_v(a.x + duw, Hpar, fpar);
                     }
                     const float4 p0 = seg[iv][kk][0], p1 = seg[iv][kk][1];
                     S[0] = fmaf(w, p0.x, S[0]);
@@ -808,7 +814,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
 }
 
 template <bool FAN, bool FBP, int SEG, int VB>
-__global__ void __launch_bounds__(kBwdTile * kBwdTile)
+__global__ void __launch_bounds__(kBwdTile * kBwdTile, CTPRJ_BWD_MINBLOCKS)
 k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
 {
     __shared__ TiledSmem<FAN, SEG, VB> sm;
