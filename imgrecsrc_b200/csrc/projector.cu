@@ -41,10 +41,10 @@ namespace ctprj {
 #define CTPRJ_FWD_VIEWS 4
 #endif
 #ifndef CTPRJ_FWD_MINBLOCKS
-#define CTPRJ_FWD_MINBLOCKS 7
+#define CTPRJ_FWD_MINBLOCKS 6
 #endif
 #ifndef CTPRJ_BWD_MINBLOCKS
-#define CTPRJ_BWD_MINBLOCKS 5
+#define CTPRJ_BWD_MINBLOCKS 4
 #endif
 constexpr int kFwdViews = CTPRJ_FWD_VIEWS;
 constexpr int kFwdThreads = 32 * kFwdViews;
@@ -217,27 +217,17 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
             const float xl = fmaf(-yf, Slf, Alf), xr = fmaf(-yf, Srf, Arf);
             // nearest pixel to each edge; exact half-way ties (where the
             // reference rounds away from zero) only decide pixels whose
-            // footprint just touches the beam edge, with weight zero
-            int x0 = __float2int_rn(fmaxf(xl, (float)(-half - 1)));
-            int x1 = __float2int_rn(fminf(xr, (float)(half + 1)));
-            x0 = max(x0, -half);
-            x1 = min(x1, half);
+            // footprint just touches the beam edge, with weight zero; the
+            // conversion saturates, so far-out edges clamp
+            const int x0 = max(__float2int_rn(xl), -half);
+            const int x1 = min(__float2int_rn(xr), half);
             if (x0 > x1) return;
             // distance of pixel (x0, y) from the ray, in FP64 then rounded;
             // distances and half beam widths in units of the footprint's ramp
             const float r0 = (float)fma((double)x0, cR, fma((double)y, sR, -off)) * fp.iw;
             const float hb0 = (FAN ? 0.5f * fmaf(fmaf((float)x0, sTf, -yf * cTf), kbw, bwc)
                                    : 0.5f * g.beamWidthF) * fp.iw;
-            for (int x = x0; x <= x1; ++x) {
-                const float jf = (float)(x - x0);
-                const float D = fmaf(jf, cRw, r0);
-                const float H = FAN ? fmaf(jf, dhbw, hb0) : hb0;
-                const float w = footprint_weight_v(D, H, fp);
-                if (MODE == kModeCount) {
-                    nz += (w != 0.0f);
-                    continue;
-                }
-                const float4 pp = __ldg(q + x), pm = __ldg(q - x);
+            auto accumulate = [&](const float w, const float4 pp, const float4 pm) {
                 const float ap = NEG ? pp.y : pp.x, am = NEG ? pm.y : pm.x;   // I(+-x, y)
                 const float bp = NEG ? pp.x : pp.y, bm = NEG ? pm.x : pm.y;   // I(+-x, -y)
                 const float cp = NEG ? pp.w : pp.z, cm = NEG ? pm.w : pm.z;   // I(y, +-x)
@@ -250,6 +240,26 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
                 S[3] = fmaf(w, cm, S[3]);
                 S[1] = fmaf(w, dp, S[1]);
                 S[7] = fmaf(w, dm, S[7]);
+            };
+            // two pixels per step, their four gathers issued together (the
+            // second pixel of an odd-length run re-reads x1 and is skipped)
+            for (int x = x0; x <= x1; x += 2) {
+                const bool two = x < x1;
+                const int xb = two ? x + 1 : x;
+                const float jf = (float)(x - x0);
+                const float D0 = fmaf(jf, cRw, r0), D1 = D0 + cRw;
+                const float H0 = FAN ? fmaf(jf, dhbw, hb0) : hb0;
+                const float H1 = FAN ? H0 + dhbw : hb0;
+                if (MODE == kModeCount) {
+                    nz += (footprint_weight_v(D0, H0, fp) != 0.0f);
+                    if (two) nz += (footprint_weight_v(D1, H1, fp) != 0.0f);
+                    continue;
+                }
+                const float4 pp0 = __ldg(q + x), pm0 = __ldg(q - x);
+                const float4 pp1 = __ldg(q + xb), pm1 = __ldg(q - xb);
+                const float w0 = footprint_weight_v(D0, H0, fp);
+                accumulate(w0, pp0, pm0);
+                if (two) accumulate(footprint_weight_v(D1, H1, fp), pp1, pm1);
             }
         };
         {
@@ -621,6 +631,7 @@ struct TileView {
     float cT, sT;
     float ucf, qec;       // u of the centre; d - v of the centre
     float hw;             // parallel: (|cos| + |sin|) / 2
+    float A, B;           // fan: (cos + sin) / 2, (cos - sin) / 2 (pixel corner offsets)
     int klo, nseg;
 };
 
@@ -629,10 +640,11 @@ template <bool FAN, int SEG, int VB>
 struct TiledSmem {
     float4 ra[VB][SEG];                      // D, cos B, sin B, half beam / qe; all / w
     float4 rb[FAN ? VB : 1][FAN ? SEG : 1];  // footprint: hw, tb, c1, rho
-    // the eight (sixteen) mirrored samples of a staged ray, contiguous: two
-    // (four) 16-byte reads per detector and pixel
-    float4 seg[VB][SEG][2];
-    float4 seg2[FAN ? 1 : VB][FAN ? 1 : SEG][2];
+    // the eight (sixteen) mirrored samples of a staged ray as two (four)
+    // float4 planes: two (four) 16-byte reads per detector and pixel, and
+    // consecutive detectors in consecutive banks
+    float4 seg[VB][2][SEG];
+    float4 seg2[FAN ? 1 : VB][2][FAN ? 1 : SEG];
     TileView tv[VB];
     FootprintV pfs[VB];
 };
@@ -668,7 +680,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     const double xc = tx * kBwdTile + 0.5 * (kBwdTile - 1), yc = ty * kBwdTile + 0.5 * (kBwdTile - 1);
     const float dx = (float)(x - xc), dy = (float)(y - yc);
     const int dmax = (g.W - 1) / 2, pC = g.pC;
-    const float invdS = (float)(1.0 / g.dSize), dF = g.dF;
+    const float invdS = (float)(1.0 / g.dSize), dFs = (float)((double)g.dF / g.dSize);
     const float hbpar = 0.5f * g.beamWidthF;
     float S[8];
 #pragma unroll
@@ -689,6 +701,8 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
             t.ucf = (float)t.uc;
             t.qec = (float)(g.d - t.vc);
             t.hw = 0.5f * (fabsf(bv.cf) + fabsf(bv.sf));
+            t.A = 0.5f * (bv.cf + bv.sf);
+            t.B = 0.5f * (bv.cf - bv.sf);
             t.klo = sp.klo;
             t.nseg = min(sp.nseg, SEG);   // the plan chose SEG above every span
             tv[iv] = t;
@@ -726,16 +740,16 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     const int row = bv.row[j];
                     v[j] = row >= 0 ? __ldg(sino + row + pC + (j < 4 ? dt : -dt)) : 0.0f;
                 }
-                seg[iv][kk][0] = make_float4(v[0], v[1], v[2], v[3]);
-                seg[iv][kk][1] = make_float4(v[4], v[5], v[6], v[7]);
+                seg[iv][0][kk] = make_float4(v[0], v[1], v[2], v[3]);
+                seg[iv][1][kk] = make_float4(v[4], v[5], v[6], v[7]);
                 if (!FAN) {   // the point-reflected detectors of the opposite view
 #pragma unroll
                     for (int j = 0; j < 8; ++j) {
                         const int row2 = bv.row2[j];
                         v[j] = row2 >= 0 ? __ldg(sino + row2 + pC - (j < 4 ? dt : -dt)) : 0.0f;
                     }
-                    seg2[FAN ? 0 : iv][FAN ? 0 : kk][0] = make_float4(v[0], v[1], v[2], v[3]);
-                    seg2[FAN ? 0 : iv][FAN ? 0 : kk][1] = make_float4(v[4], v[5], v[6], v[7]);
+                    seg2[FAN ? 0 : iv][0][FAN ? 0 : kk] = make_float4(v[0], v[1], v[2], v[3]);
+                    seg2[FAN ? 0 : iv][1][FAN ? 0 : kk] = make_float4(v[4], v[5], v[6], v[7]);
                 }
             }
         }
@@ -749,27 +763,27 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                 const float u = t.ucf + du;
                 float tlo, thi, qe = 0.0f;
                 if (FAN) {
-                    // the pixel's corner shadows (prj/cpuPrj.c:218-244); only
-                    // which detector each edge falls in matters here
+                    // the pixel's corner shadows (prj/cpuPrj.c:218-244), in
+                    // detector units; only which detector each edge falls in
+                    // matters here
                     qe = t.qec - dv;
-                    const float hc = 0.5f * t.cT, hs = 0.5f * t.sT;
-                    const float A = hc + hs, B = hc - hs;
-                    const float t0 = __fdividef(dF * (u - A), qe + B);
-                    const float t1 = __fdividef(dF * (u + B), qe + A);
-                    const float t2 = __fdividef(dF * (u + A), qe - B);
-                    const float t3 = __fdividef(dF * (u - B), qe - A);
+                    const float A = t.A, B = t.B;
+                    const float t0 = __fdividef(dFs * (u - A), qe + B);
+                    const float t1 = __fdividef(dFs * (u + B), qe + A);
+                    const float t2 = __fdividef(dFs * (u + A), qe - B);
+                    const float t3 = __fdividef(dFs * (u - B), qe - A);
                     tlo = fminf(fminf(t0, t1), fminf(t2, t3));
                     thi = fmaxf(fmaxf(t0, t1), fmaxf(t2, t3));
                 } else {
-                    tlo = u - t.hw;
-                    thi = u + t.hw;
+                    tlo = (u - t.hw) * invdS;
+                    thi = (u + t.hw) * invdS;
                 }
-                const float lim = (float)dmax + 1.0f;
-                int dl = __float2int_rn(fminf(fmaxf(tlo * invdS, -lim), lim));
-                int dr = __float2int_rn(fminf(fmaxf(thi * invdS, -lim), lim));
+                // float-to-int conversion saturates, so far-out shadows clamp
+                int dl = __float2int_rn(tlo);
+                int dr = __float2int_rn(thi);
                 dl = max(max(dl, -dmax) - t.klo, 0);
                 dr = min(min(dr, dmax) - t.klo, t.nseg - 1);
-                const float fbpw = FBP ? __fdividef(dF, qe) * __fdividef(dF, qe) : 1.0f;
+                const float fbpw = FBP ? __fdividef(g.dF, qe) * __fdividef(g.dF, qe) : 1.0f;
                 const FootprintV fpar = FAN ? FootprintV{} : pfs[iv];
                 const float duw = FAN ? 0.0f : du * fpar.iw, Hpar = FAN ? 0.0f : hbpar * fpar.iw;
                 for (int kk = dl; kk <= dr; ++kk) {
@@ -784,7 +798,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     } else {
                         w = footprint_weight_v(a.x + duw, Hpar, fpar);
                     }
-                    const float4 p0 = seg[iv][kk][0], p1 = seg[iv][kk][1];
+                    const float4 p0 = seg[iv][0][kk], p1 = seg[iv][1][kk];
                     S[0] = fmaf(w, p0.x, S[0]);
                     S[1] = fmaf(w, p0.y, S[1]);
                     S[2] = fmaf(w, p0.z, S[2]);
@@ -794,8 +808,8 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     S[6] = fmaf(w, p1.z, S[6]);
                     S[7] = fmaf(w, p1.w, S[7]);
                     if (!FAN) {
-                        const float4 q0 = seg2[FAN ? 0 : iv][FAN ? 0 : kk][0];
-                        const float4 q1 = seg2[FAN ? 0 : iv][FAN ? 0 : kk][1];
+                        const float4 q0 = seg2[FAN ? 0 : iv][0][FAN ? 0 : kk];
+                        const float4 q1 = seg2[FAN ? 0 : iv][1][FAN ? 0 : kk];
                         S[0] = fmaf(w, q0.x, S[0]);
                         S[1] = fmaf(w, q0.y, S[1]);
                         S[2] = fmaf(w, q0.z, S[2]);
