@@ -82,6 +82,7 @@ struct BwdParams {
     int tiles_side;
     int zero_axes;            // even n: row 0 and column 0 written as zero
     float scale;              // output scale: FBP PI_f/np/dSize^2, BHC gradient Ts, else 1
+    int fast_shadow;          // fan: pixel shadows from the first-order expansion (staged kernel)
     const BwdView *view;
     const DetEntry *det;
 };

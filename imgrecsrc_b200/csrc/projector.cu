@@ -631,7 +631,7 @@ struct TileView {
     float cT, sT;
     float ucf, qec;       // u of the centre; d - v of the centre
     float hw;             // parallel: (|cos| + |sin|) / 2
-    float A, B;           // fan: (cos + sin) / 2, (cos - sin) / 2 (pixel corner offsets)
+    float A, B, AB;       // fan: (cos + sin) / 2, (cos - sin) / 2 (pixel corner offsets), A B
     int klo, nseg;
 };
 
@@ -703,6 +703,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
             t.hw = 0.5f * (fabsf(bv.cf) + fabsf(bv.sf));
             t.A = 0.5f * (bv.cf + bv.sf);
             t.B = 0.5f * (bv.cf - bv.sf);
+            t.AB = t.A * t.B;
             t.klo = sp.klo;
             t.nseg = min(sp.nseg, SEG);   // the plan chose SEG above every span
             tv[iv] = t;
@@ -768,12 +769,23 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     // matters here
                     qe = t.qec - dv;
                     const float A = t.A, B = t.B;
-                    const float t0 = __fdividef(dFs * (u - A), qe + B);
-                    const float t1 = __fdividef(dFs * (u + B), qe + A);
-                    const float t2 = __fdividef(dFs * (u + A), qe - B);
-                    const float t3 = __fdividef(dFs * (u - B), qe - A);
-                    tlo = fminf(fminf(t0, t1), fminf(t2, t3));
-                    thi = fmaxf(fmaxf(t0, t1), fmaxf(t2, t3));
+                    if (p.fast_shadow) {
+                        // corner i at (u + du_i, qe + dq_i): t_i = K (u + du_i) / (1 + r dq_i)
+                        // ~ K (u + du_i - rho dq_i - r du_i dq_i), K = d r, rho = r u; the
+                        // corners pair up as u + c +- a1 and u - c +- a2
+                        const float r = __fdividef(1.0f, qe), rho = r * u, c = r * t.AB;
+                        const float a1 = fabsf(fmaf(rho, B, A)), a2 = fabsf(fmaf(-rho, A, B));
+                        const float K = dFs * r;
+                        tlo = K * (u + fminf(c - a1, -c - a2));
+                        thi = K * (u + fmaxf(c + a1, a2 - c));
+                    } else {
+                        const float t0 = __fdividef(dFs * (u - A), qe + B);
+                        const float t1 = __fdividef(dFs * (u + B), qe + A);
+                        const float t2 = __fdividef(dFs * (u + A), qe - B);
+                        const float t3 = __fdividef(dFs * (u - B), qe - A);
+                        tlo = fminf(fminf(t0, t1), fminf(t2, t3));
+                        thi = fmaxf(fmaxf(t0, t1), fmaxf(t2, t3));
+                    }
                 } else {
                     tlo = (u - t.hw) * invdS;
                     thi = (u + t.hw) * invdS;
@@ -847,6 +859,22 @@ static BwdParams bwd_params(const ctprj_plan *pl, int fbp, float scale)
                   : scale;
     p.view = pl->d_bview;
     p.det = pl->d_det;
+    // The staged fan kernel may bound a pixel's shadow from 1/qe and a first-
+    // order expansion in (pixel half-diagonal) / qe instead of four divisions
+    // when the dropped second-order terms stay below 1e-4 detector: at most
+    //   K (h + 1) r^2 / 2,  r = 1 / (d - h),  K = d r / dSize,
+    // h = the image's half-diagonal.  Detectors that the exact and the
+    // bounded shadow disagree on lie within that distance of a shadow edge,
+    // where the footprint weight is of the order of its square.
+    p.fast_shadow = 0;
+    if (pl->g.fan) {
+        const double h = (pl->g.half + 0.5) * 1.4142135623730951 + 1.0;
+        const double d = pl->g.d;
+        if (d > 2.0 * h) {
+            const double r = 1.0 / (d - h), K = d * r / pl->g.dSize;
+            p.fast_shadow = K * (h + 1.0) * r * r * 0.5 <= 1e-4;
+        }
+    }
     return p;
 }
 
