@@ -118,6 +118,9 @@ def lib():
         "ctprj_stream_flags_create": ([ctypes.c_int, ctypes.POINTER(VP), ctypes.POINTER(VP)], ctypes.c_int),
         "ctprj_stream_flags_destroy": ([VP], None),
         "ctprj_batch_stream_backward": ([VP, VP, ctypes.c_double, VP, VP], ctypes.c_int),
+        "ctprj_masked_forward": ([VP, VP, ctypes.c_longlong, VP, ctypes.c_double, VP, VP], ctypes.c_int),
+        "ctprj_masked_backward": ([VP, VP, ctypes.c_longlong, VP, ctypes.c_double, VP, VP], ctypes.c_int),
+        "ctprj_masked_fbp": ([VP, VP, ctypes.c_longlong, VP, ctypes.c_double, VP, VP], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

@@ -32,7 +32,8 @@ def sources():
 def _compile(src, verbose):
     obj = os.path.join(OBJ, os.path.basename(src)[:-3] + ".o")
     deps = [src] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".cuh"))]
-    deps.append(os.path.join(os.path.dirname(PKG), "include", "ctprj.h"))
+    inc = os.path.join(os.path.dirname(PKG), "include")
+    deps += [os.path.join(inc, h) for h in os.listdir(inc) if h.endswith(".h")]
     if os.path.exists(obj) and all(os.path.getmtime(obj) >= os.path.getmtime(d) for d in deps):
         return obj, ""
     cmd = [nvcc()] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]

@@ -119,6 +119,8 @@ static void free_plan(ctprj_plan *p)
     cudaFree(p->d_count);
     cudaFree(p->d_ramp);
     cudaFree(p->d_fsino);
+    cudaFree(p->d_mimg);
+    cudaFree(p->d_msino);
     delete p;
 }
 

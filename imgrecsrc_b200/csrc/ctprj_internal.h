@@ -129,6 +129,9 @@ struct ctprj_plan {
     // FBP: ramp-filter taps (2*prjWidth) and filtered-sinogram scratch
     float *d_ramp;
     float *d_fsino;
+    // MATLAB-layout entry points: image and sinogram scratch (allocated on first use)
+    float *d_mimg;
+    float *d_msino;
 };
 
 // polychromatic model on a plan (bhc.cu, bhc_loop.cu)

@@ -90,3 +90,59 @@ def mParPrj(x, maskIdx, conf, cmd):
                        mask.size))
     check(L.parPrjThread())
     return out
+
+
+def gpuFanParOps(projector, mask=None, Ts=1.0):
+    """Phi, Phit and FBP of ConfigCT.gpuFanParOps (tomography/ConfigCT.m:122-135)
+    with its mask (utils/maskFunc.m), as device operators on float64 torch
+    tensors in MATLAB's layout:
+      Phi(s)  = Ts * gpuPrj(maskFunc(s, maskIdx, [n n]), 0, 'forward')
+      Phit(y) = Ts * maskFunc(gpuPrj(y, 0, 'backward'), maskIdx)
+      FBP(y)  = maskFunc(gpuPrj(y, 0, 'FBP'), maskIdx) / Ts
+    mask: an n x n array (nonzero = reconstructed pixel, MATLAB's rows and
+    columns) or None for the whole image.  s is the vector of masked pixels in
+    column-major order, y the view-major sinogram vector.  The scatter, gather,
+    transposes and casts run as kernels (include/ctprj_masked.h)."""
+    import torch
+
+    from ._lib import lib as _l
+    g = projector.geometry
+    dev = torch.device("cuda", projector.device)
+    if mask is None:
+        d_mask, npix = None, g.n * g.n
+    else:
+        m = np.asarray(mask)
+        idx = np.flatnonzero(m.ravel(order="F")).astype(np.int32)   # find(mask ~= 0) - 1
+        d_mask = torch.from_numpy(idx).to(dev)
+        npix = int(idx.size)
+    nsino = g.np * g.prjWidth
+    mptr = None if d_mask is None else ctypes.c_void_p(d_mask.data_ptr())
+
+    def _vec(t, size):
+        if t.dtype != torch.float64 or t.device != dev or t.numel() != size or not t.is_contiguous():
+            raise ValueError("expected a contiguous float64 CUDA vector of %d values" % size)
+        return ctypes.c_void_p(t.data_ptr())
+
+    def _stream():
+        return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+    def Phi(s):
+        y = torch.empty(nsino, dtype=torch.float64, device=dev)
+        check(_l().ctprj_masked_forward(projector._plan, mptr, npix, _vec(s, npix), float(Ts),
+                                        _vec(y, nsino), _stream()))
+        return y
+
+    def Phit(y):
+        s = torch.empty(npix, dtype=torch.float64, device=dev)
+        check(_l().ctprj_masked_backward(projector._plan, mptr, npix, _vec(y, nsino), float(Ts),
+                                         _vec(s, npix), _stream()))
+        return s
+
+    def FBP(y):
+        s = torch.empty(npix, dtype=torch.float64, device=dev)
+        check(_l().ctprj_masked_fbp(projector._plan, mptr, npix, _vec(y, nsino), 1.0 / float(Ts),
+                                    _vec(s, npix), _stream()))
+        return s
+
+    Phi.mask = d_mask
+    return Phi, Phit, FBP
