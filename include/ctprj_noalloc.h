@@ -6,9 +6,10 @@
  * cannot call cudaMalloc -- code running inside another framework's memory
  * pool or allocator, real-time loops that must not block on allocation, or
  * embedders that have reserved the whole GPU.  It calls no cudaMalloc, no
- * cudaFree and no allocating library routine; its scratch (the transposed
- * image and the ray tables, about 4.4 MiB) is a set of file-scope device arrays
- * that every GPU loading the library holds until the process exits.
+ * cudaFree and no allocating library routine; its scratch (the forward pass's
+ * quad image -- the eight symmetric copies of each pixel, twice the image's
+ * size -- and the ray tables, about 8.5 MiB) is a set of file-scope device
+ * arrays that every GPU loading the library holds until the process exits.
  */
 #ifndef CTPRJ_NOALLOC_H
 #define CTPRJ_NOALLOC_H
