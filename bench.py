@@ -41,6 +41,9 @@ L2_FLUSH_BYTES = 512 << 20   # > 126 MB L2
 # phantom (0 / 2.7 / 7.8 g/cm^3), J = 30 b1 coefficients on kappa log-spaced over
 # [1e-2, 1e2] cm^2/g, Poisson counts at I0 = 1e5 per ray, 2 cm field of view
 BHC = dict(J=30, I0=1e5, fov_cm=2.0)
+# the polychromatic model's own configuration: fan 1024^2, 720 views over
+# [0, 2 pi), 1024 detectors, source 2048 px from the isocentre
+BHC_WORKLOAD = dict(n=1024, prjWidth=1024, np=720, prjFull=720, dSize=1.0, effectiveRate=1.0, d=2048.0)
 
 
 def geometry_tuple(w):
@@ -264,7 +267,15 @@ def our_arm(args):
     achieved = kbytes / (kms * 1e-3) / 1e9
     traffic = profiled_traffic().get("k_backward_tiled<fan>" if bwd_ms >= fwd_ms else "k_forward<fan>")
 
-    bhc_line = bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
+    # BHC gradient iterations on the polychromatic model's own configuration
+    # (fan 1024^2, 720 views, 1024 bins, J = 20) and on the 2048^2 geometry
+    g3 = ct.Geometry(*geometry_tuple(BHC_WORKLOAD))
+    pr3 = ct.Projector(g3, device=local)
+    bhc_line = {"fan_1024": bhc_leg(ct, g3, pr3, flush, stream, max(3, args.steps // 2), 20,
+                                    "fan 1024^2, 720 views/[0,2pi), 1024 bins, d=2048 px"),
+                "fan_2048": bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2), BHC["J"],
+                                    "fan 2048^2, 1440 views, 2048 bins, d=8192 px")}
+    pr3.close()
     batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
     loop_line = loop_leg(ct, g, pr, args.loop_iters) if args.loop_iters > 0 else None
 
@@ -324,7 +335,7 @@ def our_arm(args):
         print(json.dumps(line), flush=True)
 
 
-def bhc_leg(ct, g, pr, flush, stream, steps):
+def bhc_leg(ct, g, pr, flush, stream, steps, J, workload):
     """BHC gradient iterations per second: the fused forward (projection with
     the spline epilogue) + adjoint, against the plain FP32 projector path in
     the reference's call structure (bhc/beamhardenSpline.m:382-447: Phi(alpha),
@@ -335,7 +346,7 @@ def bhc_leg(ct, g, pr, flush, stream, steps):
     import torch
 
     from imgrecsrc_b200 import bhc, phantom
-    J, I0 = BHC["J"], BHC["I0"]
+    I0 = BHC["I0"]
     Ts = BHC["fov_cm"] / g.n
     x = torch.from_numpy(phantom.two_material_phantom(g.n, seed=2)).cuda()
     nodes = bhc.kappa_nodes(J)
@@ -366,8 +377,8 @@ def bhc_leg(ct, g, pr, flush, stream, steps):
         model.terms(s1, Ie, imea, save=True)
         return model.backward()
 
-    out = {"workload": "fan 2048^2, 1440 views, 2048 bins, d=8192 px; two-material phantom; "
-                       "J=30 b1 spectrum on [1e-2,1e2] cm^2/g; Poisson counts I0=1e5; Ts=%g cm" % Ts,
+    out = {"workload": "%s; two-material phantom; J=%d b1 spectrum on [1e-2,1e2] cm^2/g; "
+                       "Poisson counts I0=1e5; Ts=%g cm" % (workload, J, Ts),
            "iteration": "f (FP64) + df/dx + df/dIe"}
     for name, fn in (("fused", fused), ("plain", plain_ref), ("plain_min", plain_min)):
         for _ in range(2):

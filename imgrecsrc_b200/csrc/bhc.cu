@@ -41,7 +41,7 @@ __device__ __forceinline__ double block_sum_any(double v, double *red)
 constexpr int kSpecChunk = 8;
 
 __global__ void __launch_bounds__(kSpecThreads)
-k_bhc_spectrum(const float *__restrict__ s, const float *__restrict__ r, long long nrays,
+k_bhc_spectrum(const float *__restrict__ s, const double *__restrict__ r, long long nrays,
                const double *__restrict__ tab_g, int J, double *__restrict__ part)
 {
     __shared__ double tab[kMaxJ * kSplStride];
@@ -56,7 +56,7 @@ k_bhc_spectrum(const float *__restrict__ s, const float *__restrict__ r, long lo
         const double *t0 = tab + j0 * kSplStride;
         for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
              i += (long long)gridDim.x * blockDim.x) {
-            const double si = (double)s[i], ri = (double)r[i];
+            const double si = (double)s[i], ri = r[i];
             const double is2 = 1.0 / (si * si), as = fabs(si);
             double eL = exp(-t0[0] * si), eC = exp(-t0[1] * si);
 #pragma unroll
@@ -109,7 +109,7 @@ k_bhc_terms(const float *__restrict__ sino, long long nrays, BhcArgs a)
         if (a.w_out) {
             a.w_out[i] = (float)(t.r * e.sBL);
             a.s_out[i] = (float)s;
-            a.r_out[i] = (float)t.r;
+            a.r_out[i] = t.r;
         }
         f += t.f;
     }
@@ -284,7 +284,7 @@ extern "C" int ctprj_bhc_create(ctprj_plan *plan, int J, const double *kappa_nod
         (st = cuda_error(cudaMemcpy(m->d_tab2, tab2.data(), sizeof(double) * tab2.size(),
                                     cudaMemcpyHostToDevice), "spline upload")) ||
         (st = cuda_error(cudaMalloc((void **)&m->d_s, sizeof(float) * nr), "ray state")) ||
-        (st = cuda_error(cudaMalloc((void **)&m->d_r, sizeof(float) * nr), "ray state")) ||
+        (st = cuda_error(cudaMalloc((void **)&m->d_r, sizeof(double) * nr), "ray state")) ||
         (st = cuda_error(cudaMalloc((void **)&m->d_w, sizeof(float) * nr), "ray state"))) {
         cudaFree(m->d_tab); cudaFree(m->d_tab2); cudaFree(m->d_s); cudaFree(m->d_r); cudaFree(m->d_w);
         delete m;
@@ -442,7 +442,7 @@ extern "C" int ctprj_bhc_hessian(ctprj_bhc *m, const double *d_Ie, const float *
     return CTPRJ_OK;
 }
 
-extern "C" int ctprj_bhc_state(ctprj_bhc *m, const float **d_s, const float **d_r, const float **d_w)
+extern "C" int ctprj_bhc_state(ctprj_bhc *m, const float **d_s, const double **d_r, const float **d_w)
 {
     if (!m) return set_error(CTPRJ_EINVAL, "NULL model");
     if (d_s) *d_s = m->d_s;

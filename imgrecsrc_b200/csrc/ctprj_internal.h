@@ -60,7 +60,9 @@ struct BhcArgs {
     int J;
     double Ts;                // pixel size: s = Ts * (A x)
     const float *imea;        // measured intensity / I0 per ray (np * prjWidth)
-    float *s_out, *r_out, *w_out;   // per-ray s, r = df/dBL, r dBL/ds; NULL: not kept
+    float *s_out, *w_out;     // per-ray s and r dBL/ds (the backprojected weight); NULL: not kept
+    double *r_out;            // per-ray r = df/dBL in FP64: the spectrum gradient sums it over
+                              // all rays with cancellation, which single precision would not survive
     double *part;             // per-block partial sums of the likelihood terms
     int noise;                // kNoisePoisson or kNoiseGaussian
 };
@@ -140,7 +142,8 @@ struct ctprj_bhc {
     int J;
     double Ts;
     double *d_tab;            // spline table, J * kSplStride doubles
-    float *d_s, *d_r, *d_w;   // per-ray state, np * prjWidth each
+    float *d_s, *d_w;         // per-ray state, np * prjWidth each
+    double *d_r;
     double *d_part;           // per-block partials
     int part_cap;             // doubles in d_part
     int saved;                // the per-ray state holds the last forward's values

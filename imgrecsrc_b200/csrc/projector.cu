@@ -116,7 +116,7 @@ __device__ __forceinline__ double bhc_entry(const BhcArgs &a, const double *tab,
     if (a.w_out) {
         a.w_out[idx] = (float)(t.r * e.sBL);
         a.s_out[idx] = (float)s;
-        a.r_out[idx] = (float)t.r;
+        a.r_out[idx] = t.r;
     }
     return t.f;
 }

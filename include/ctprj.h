@@ -136,7 +136,7 @@ int ctprj_count_updates(ctprj_plan *plan, long long *fwd, long long *bwd, void *
 typedef struct ctprj_bhc ctprj_bhc;
 
 /* J in [1, 32]; kappa_nodes: J + 2 increasing positive nodes (cm^2/g);
- * Ts > 0: pixel size (cm).  Allocates per-ray state (3 floats per ray). */
+ * Ts > 0: pixel size (cm).  Allocates per-ray state (2 floats and 1 double per ray). */
 int ctprj_bhc_create(ctprj_plan *plan, int J, const double *kappa_nodes, double Ts,
                      ctprj_bhc **model);
 void ctprj_bhc_destroy(ctprj_bhc *model);
@@ -164,10 +164,10 @@ int ctprj_bhc_terms(ctprj_bhc *model, const float *d_sino, const double *d_Ie,
  * solvers that work on the matrix. */
 int ctprj_bhc_basis(ctprj_bhc *model, const float *d_sino, double *d_A, void *stream);
 
-/* Device pointers of the saved per-ray state: s_i, r_i = df/dBL_i
- * (1 - m_i/BL_i for the Poisson model) and r_i dBL/ds (np*prjWidth floats
- * each). */
-int ctprj_bhc_state(ctprj_bhc *model, const float **d_s, const float **d_r, const float **d_w);
+/* Device pointers of the saved per-ray state (np*prjWidth entries each): s_i
+ * (float), r_i = df/dBL_i (double; 1 - m_i/BL_i for the Poisson model) and
+ * r_i dBL/ds (float). */
+int ctprj_bhc_state(ctprj_bhc *model, const float **d_s, const double **d_r, const float **d_w);
 
 /* Noise model of the likelihood.  CTPRJ_NOISE_POISSON (the default):
  * bhc/poissLAlpha.m, bhc/poissLI.m as above.  CTPRJ_NOISE_GAUSSIAN: the
