@@ -798,7 +798,8 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                 const float fbpw = FBP ? __fdividef(g.dF, qe) * __fdividef(g.dF, qe) : 1.0f;
                 const FootprintV fpar = FAN ? FootprintV{} : pfs[iv];
                 const float duw = FAN ? 0.0f : du * fpar.iw, Hpar = FAN ? 0.0f : hbpar * fpar.iw;
-                for (int kk = dl; kk <= dr; ++kk) {
+                // the weight of staged detector kk for this pixel
+                auto weight = [&](const int kk) {
                     const float4 a = ra[iv][kk];
                     float w;
                     if (FAN) {
@@ -810,7 +811,9 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     } else {
                         w = footprint_weight_v(a.x + duw, Hpar, fpar);
                     }
-                    const float4 p0 = seg[iv][0][kk], p1 = seg[iv][1][kk];
+                    return w;
+                };
+                auto accumulate = [&](const float w, const float4 p0, const float4 p1) {
                     S[0] = fmaf(w, p0.x, S[0]);
                     S[1] = fmaf(w, p0.y, S[1]);
                     S[2] = fmaf(w, p0.z, S[2]);
@@ -819,17 +822,22 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     S[5] = fmaf(w, p1.y, S[5]);
                     S[6] = fmaf(w, p1.z, S[6]);
                     S[7] = fmaf(w, p1.w, S[7]);
-                    if (!FAN) {
-                        const float4 q0 = seg2[FAN ? 0 : iv][0][FAN ? 0 : kk];
-                        const float4 q1 = seg2[FAN ? 0 : iv][1][FAN ? 0 : kk];
-                        S[0] = fmaf(w, q0.x, S[0]);
-                        S[1] = fmaf(w, q0.y, S[1]);
-                        S[2] = fmaf(w, q0.z, S[2]);
-                        S[3] = fmaf(w, q0.w, S[3]);
-                        S[4] = fmaf(w, q1.x, S[4]);
-                        S[5] = fmaf(w, q1.y, S[5]);
-                        S[6] = fmaf(w, q1.z, S[6]);
-                        S[7] = fmaf(w, q1.w, S[7]);
+                };
+                // two detectors per step, their shared-memory reads issued
+                // together (the second of an odd-length run re-reads dr and is
+                // skipped); per sum the order of the terms is unchanged
+                for (int kk = dl; kk <= dr; kk += 2) {
+                    const bool two = kk < dr;
+                    const int kb = two ? kk + 1 : kk;
+                    const float4 p0 = seg[iv][0][kk], p1 = seg[iv][1][kk];
+                    const float4 r0 = seg[iv][0][kb], r1 = seg[iv][1][kb];
+                    const float w0 = weight(kk);
+                    const float w1 = weight(kb);
+                    accumulate(w0, p0, p1);
+                    if (!FAN) accumulate(w0, seg2[FAN ? 0 : iv][0][FAN ? 0 : kk], seg2[FAN ? 0 : iv][1][FAN ? 0 : kk]);
+                    if (two) {
+                        accumulate(w1, r0, r1);
+                        if (!FAN) accumulate(w1, seg2[FAN ? 0 : iv][0][FAN ? 0 : kb], seg2[FAN ? 0 : iv][1][FAN ? 0 : kb]);
                     }
                 }
             }
