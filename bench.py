@@ -277,7 +277,15 @@ def our_arm(args):
                                     "fan 2048^2, 1440 views, 2048 bins, d=8192 px")}
     pr3.close()
     batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
-    loop_line = loop_leg(ct, g, pr, args.loop_iters) if args.loop_iters > 0 else None
+    loop_line = None
+    if args.loop_iters > 0:
+        if args.loop_geometry == "1024":
+            gl = ct.Geometry(*geometry_tuple(BHC_WORKLOAD))
+            prl = ct.Projector(gl, device=local)
+            loop_line = loop_leg(ct, gl, prl, args.loop_iters)
+            prl.close()
+        else:
+            loop_line = loop_leg(ct, g, pr, args.loop_iters)
 
     # end to end through the reference-facing C ABI: setup() once, then per
     # step gpuPrj(FWD) and gpuPrj(BWD) on pinned host buffers (every call
@@ -405,7 +413,7 @@ def bhc_leg(ct, g, pr, flush, stream, steps, J, workload):
 
 
 def loop_leg(ct, g, pr, iters):
-    """The alternating BHC reconstruction at 2048^2 (J = 30, Poisson counts at
+    """The alternating BHC reconstruction on geometry g (J = 30, Poisson counts at
     I0 = 1e5): `iters` iterations of a projected-gradient density step
     (npg/PG.m with the projection on x >= 0, majorisation line search) and an
     FP64 non-negative spectrum step (Newton with an active-set QP on Ie >= 0),
@@ -427,8 +435,9 @@ def loop_leg(ct, g, pr, iters):
     gen = torch.Generator(device="cuda").manual_seed(7)
     imea = (torch.poisson(I0 * BL, generator=gen) / I0).float().contiguous()
     del A, BL
-    out = {"workload": "fan 2048^2, 1440 views, 2048 bins, d=8192; J=30; I0=1e5; start x=1 g/cm^3, "
-                       "Ie uniform; %d iterations of density step + spectrum step (<= 2 Newton steps)" % iters}
+    out = {"workload": "fan %d^2, %d views, %d bins, d=%g; J=30; I0=1e5; start x=1 g/cm^3, "
+                       "Ie uniform; %d iterations of density step + spectrum step (<= 2 Newton steps)"
+                       % (g.n, g.np, g.prjWidth, g.d, iters)}
     res = {}
     for name, method, unfused in (("pg_fused", "pg", False), ("pg_unfused", "pg", True),
                                   ("npg_fused", "npg", False)):
@@ -534,6 +543,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--loop-iters", type=int, default=50,
                     help="alternating BHC iterations of the reconstruction leg (0: skip)")
+    ap.add_argument("--loop-geometry", default="2048", choices=["2048", "1024"],
+                    help="reconstruction leg on the 2048^2 workload (config 5) or on the "
+                         "1024^2 configuration of the polychromatic model (smaller, for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)

@@ -33,62 +33,78 @@ constexpr int kIeChunk = 64;          // rays per shared-memory chunk
 constexpr int kIeThreads = 256;
 constexpr int kMaxH = kMaxJ * (kMaxJ + 1) / 2;
 
-// per-block partials of f, g (J) and the upper triangle of H (J(J+1)/2) for
-// Ie; layout part[block * (1 + J + J(J+1)/2)].  Per chunk of kIeChunk rays the
-// block stages the basis rows A_i and the curvature-scaled rows sqrt(q_i) A_i
-// in shared memory; H = sum_i (sqrt(q_i) A_i)^T (sqrt(q_i) A_i) is then a small
-// GEMM in which thread (tj, tk) of a 16 x 16 grid accumulates the 2 x 2 tile
-// of rows 2tj.. and columns 2tk.. in registers (tiles below the diagonal
-// idle), g_j = sum_i A_ij r_i is split over the eight warps, and f over the
-// rays of the first two warps.  q >= 0 for both noise models' curvatures.
-__global__ void __launch_bounds__(kIeThreads, 2)
-k_ie_eval(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
-          const double *__restrict__ Ie, int want_h, int noise, double *__restrict__ part)
+// The spectrum model at Ie from the column-major basis matrix A (J x nrays),
+// in two passes whose per-block partials share one layout,
+// part[block * (1 + J + J(J+1)/2)] = {f, g (J), upper triangle of H}:
+//  k_ie_rays  one thread per ray: Ir = A_i . Ie, the likelihood term into f,
+//             r_i = df/dIr and sqrt(q_i) (q: the model curvature, >= 0 for
+//             both noise models) into per-ray arrays;
+//  k_ie_gh    per chunk of kIeChunk rays the block stages the rows
+//             sqrt(q_i) A_i in shared memory while it accumulates
+//             g_j = sum_i A_ij r_i; H = sum_i (sqrt(q_i) A_i)^T (sqrt(q_i) A_i)
+//             is then a small GEMM in which thread (tj, tk) of a 16 x 16 grid
+//             keeps the 2 x 2 tile of rows 2tj.. and columns 2tk.. in
+//             registers (tiles below the diagonal idle).
+__global__ void __launch_bounds__(256)
+k_ie_rays(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
+          const double *__restrict__ Ie, int noise, int stride, double *__restrict__ rr,
+          double *__restrict__ sq, double *__restrict__ part)
 {
-    __shared__ __align__(16) double As[kIeChunk][kMaxJ];
-    __shared__ __align__(16) double Ss[kIeChunk][kMaxJ];
-    __shared__ double rs[kIeChunk], fs[kIeChunk];
     __shared__ double Is[kMaxJ];
-    __shared__ double gpart[kIeThreads / 32][kMaxJ];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    for (int j = t; j < kMaxJ; j += blockDim.x) Is[j] = j < J ? Ie[j] : 0.0;
-    const int tj = t >> 4, tk = t & 15;
-    const bool htile = want_h && 2 * tj <= 2 * tk + 1 && 2 * tj < J && 2 * tk < J;
-    double h00 = 0.0, h01 = 0.0, h10 = 0.0, h11 = 0.0;
-    double f = 0.0, g = 0.0;
+    __shared__ double red[8];
+    for (int j = threadIdx.x; j < J; j += blockDim.x) Is[j] = Ie[j];
     __syncthreads();
+    double f = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
+         i += (long long)gridDim.x * blockDim.x) {
+        double Ir = 0.0;
+        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + (size_t)j * nrays + i), Is[j], Ir);
+        const double mi = (double)m[i];
+        const RayTerms t = ray_terms(noise, Ir, mi);
+        f += t.f;
+        rr[i] = t.r;
+        sq[i] = sqrt(ray_curvature_model(noise, Ir, mi));
+    }
+    for (int o = 16; o > 0; o >>= 1) f += __shfl_down_sync(0xffffffffu, f, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = f;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        part[(size_t)blockIdx.x * stride] = t;
+    }
+}
+
+__global__ void __launch_bounds__(kIeThreads)
+k_ie_gh(const double *__restrict__ A, long long nrays, int J, const double *__restrict__ rr,
+        const double *__restrict__ sq, int stride, double *__restrict__ part)
+{
+    // rows read as double2 and kept 16-byte aligned; stride 34 spreads the
+    // column-wise staging writes over the banks
+    __shared__ __align__(16) double Ss[kIeChunk][kMaxJ + 2];
+    __shared__ double gred[8][kIeThreads];
+    const int t = threadIdx.x;
+    const int tj = t >> 4, tk = t & 15;
+    const bool htile = 2 * tj <= 2 * tk + 1 && 2 * tj < J && 2 * tk < J;
+    // staging role: ray rs of the chunk, basis functions js + 4 q (q < 8)
+    const int rs = t % kIeChunk, js = t / kIeChunk;
+    double h00 = 0.0, h01 = 0.0, h10 = 0.0, h11 = 0.0;
+    double g[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) g[q] = 0.0;
     for (long long c0 = (long long)blockIdx.x * kIeChunk; c0 < nrays; c0 += (long long)gridDim.x * kIeChunk) {
         const int nc = (int)(nrays - c0 < kIeChunk ? nrays - c0 : kIeChunk);
+        const bool in = rs < nc;
+        const double ri = in ? rr[c0 + rs] : 0.0, si = in ? sq[c0 + rs] : 0.0;
         __syncthreads();
-        for (int e = t; e < kIeChunk * kMaxJ; e += blockDim.x) {
-            const int r = e / kMaxJ, j = e % kMaxJ;
-            As[r][j] = (r < nc && j < J) ? A[(size_t)(c0 + r) * J + j] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int j = js + 4 * q;
+            const double a = (in && j < J) ? __ldg(A + (size_t)j * nrays + c0 + rs) : 0.0;
+            g[q] = fma(a, ri, g[q]);
+            Ss[rs][j] = si * a;
         }
         __syncthreads();
-        if (t < kIeChunk) {
-            double rr = 0.0, sq = 0.0, ff = 0.0;
-            if (t < nc) {
-                double Ir = 0.0;
-                for (int j = 0; j < J; ++j) Ir = fma(As[t][j], Is[j], Ir);
-                const double mi = (double)m[c0 + t];
-                const RayTerms rt = ray_terms(noise, Ir, mi);
-                rr = rt.r;
-                ff = rt.f;
-                sq = sqrt(ray_curvature_model(noise, Ir, mi));
-            }
-            rs[t] = rr;
-            fs[t] = ff;
-            if (want_h)
-                for (int j = 0; j < kMaxJ; ++j) Ss[t][j] = sq * As[t][j];
-        }
-        __syncthreads();
-        if (warp < 2) {   // f over the chunk, a fixed order
-            double v = fs[t];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0) f += v;
-        }
-        if (lane < J)     // g: warp w takes rays w, w + 8, ...
-            for (int r = warp; r < nc; r += kIeThreads / 32) g = fma(As[r][lane], rs[r], g);
         if (htile) {
             for (int r = 0; r < nc; ++r) {
                 const double2 a = *reinterpret_cast<const double2 *>(&Ss[r][2 * tj]);
@@ -100,17 +116,15 @@ k_ie_eval(const double *__restrict__ A, const float *__restrict__ m, long long n
             }
         }
     }
+    // g: the kIeChunk threads of staging group js hold functions js + 4 q
+#pragma unroll
+    for (int q = 0; q < 8; ++q) gred[q][t] = g[q];
     __syncthreads();
-    if (lane < kMaxJ) gpart[warp][lane] = g;
-    // f: lanes 0 of warps 0 and 1 hold the two halves
-    if (lane == 0 && warp < 2) rs[warp] = f;
-    __syncthreads();
-    const int w = 1 + J + J * (J + 1) / 2;
-    double *out = part + (size_t)blockIdx.x * w;
-    if (t == 0) out[0] = rs[0] + rs[1];
+    double *out = part + (size_t)blockIdx.x * stride;
     if (t < J) {
+        const int grp = t % 4, q = t / 4;
         double gs = 0.0;
-        for (int q = 0; q < kIeThreads / 32; ++q) gs += gpart[q][t];
+        for (int u = 0; u < kIeChunk; ++u) gs += gred[q][grp * kIeChunk + u];
         out[1 + t] = gs;
     }
     if (htile) {
@@ -122,8 +136,34 @@ k_ie_eval(const double *__restrict__ A, const float *__restrict__ m, long long n
         if (j0 + 1 < J && j0 + 1 <= k0) h[(j0 + 1) * J - (j0 + 1) * j0 / 2 + (k0 - j0 - 1)] = h10;
         if (k0 + 1 < J) h[(j0 + 1) * J - (j0 + 1) * j0 / 2 + (k0 - j0)] = h11;
     }
-    if (!want_h)
-        for (int e = t; e < J * (J + 1) / 2; e += blockDim.x) out[1 + J + e] = 0.0;
+}
+
+// per-block partials of f alone (the line search's trial points), written to
+// part[block * stride]: one thread per ray, its basis values read down the
+// columns of A (coalesced across the warp)
+__global__ void __launch_bounds__(256)
+k_ie_f(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
+       const double *__restrict__ Ie, int noise, int stride, double *__restrict__ part)
+{
+    __shared__ double Is[kMaxJ];
+    __shared__ double red[8];
+    for (int j = threadIdx.x; j < J; j += blockDim.x) Is[j] = Ie[j];
+    __syncthreads();
+    double f = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
+         i += (long long)gridDim.x * blockDim.x) {
+        double Ir = 0.0;
+        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + (size_t)j * nrays + i), Is[j], Ir);
+        f += ray_terms(noise, Ir, (double)m[i]).f;
+    }
+    for (int o = 16; o > 0; o >>= 1) f += __shfl_down_sync(0xffffffffu, f, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = f;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        part[(size_t)blockIdx.x * stride] = t;
+    }
 }
 
 // out[c] = sum over blocks of part[b * stride + c] for c < ncols (fixed order, FP64)
@@ -423,7 +463,9 @@ k_axpy(const float *__restrict__ x, const float *__restrict__ g, float alpha, lo
         out[i] = fmaf(alpha, g[i], x[i]);
 }
 
-// basis matrix from the saved per-ray projections s (already scaled by Ts)
+// basis matrix from the saved per-ray projections s (already scaled by Ts),
+// column-major: A[j * nrays + i] = b_j(s_i), so that a warp's writes (and every
+// later read) of one basis function are contiguous
 __global__ void __launch_bounds__(256)
 k_basis_from_s(const float *__restrict__ s, long long nrays, const double *__restrict__ tab_g, int J,
                double *__restrict__ A)
@@ -436,13 +478,12 @@ k_basis_from_s(const float *__restrict__ s, long long nrays, const double *__res
         const double si = (double)s[i];
         const double is2 = 1.0 / (si * si), as = fabs(si);
         double eL = exp(-tab[0] * si), eC = exp(-tab[1] * si);
-        double *row = A + (size_t)i * J;
         for (int j = 0; j < J; ++j) {
             const double *t = tab + j * kSplStride;
             const double eR = exp(-t[2] * si);
             double bj = ((eC - eR) * t[4] - (eL - eC) * t[3]) * is2;
             if (as < t[9]) bj = fma(fma(fma(t[8], si, t[7]), si, t[6]), si, t[5]);
-            row[j] = bj;
+            A[(size_t)j * nrays + i] = bj;
             eL = eC;
             eC = eR;
         }
@@ -459,6 +500,7 @@ namespace {
 // reduction buffers
 struct SpectrumWs {
     double *A = nullptr, *part = nullptr, *fgh = nullptr, *dir = nullptr, *trial = nullptr, *f1 = nullptr;
+    double *rr = nullptr, *sq = nullptr;   // per-ray df/dIr and sqrt(curvature)
     int *qp_iters = nullptr;
     int blocks = 0;
     int alloc(int J, long long nr, int nblocks, cudaStream_t s)
@@ -472,7 +514,9 @@ struct SpectrumWs {
             (st = cuda_error(cudaMallocAsync((void **)&dir, sizeof(double) * J, s), "partials")) ||
             (st = cuda_error(cudaMallocAsync((void **)&trial, sizeof(double) * (J + 1), s), "partials")) ||
             (st = cuda_error(cudaMallocAsync((void **)&f1, sizeof(double) * 2, s), "partials")) ||
-            (st = cuda_error(cudaMallocAsync((void **)&qp_iters, sizeof(int), s), "partials")))
+            (st = cuda_error(cudaMallocAsync((void **)&qp_iters, sizeof(int), s), "partials")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&rr, sizeof(double) * nr, s), "ray weights")) ||
+            (st = cuda_error(cudaMallocAsync((void **)&sq, sizeof(double) * nr, s), "ray weights")))
             release(s);
         return st;
     }
@@ -485,7 +529,9 @@ struct SpectrumWs {
         if (trial) cudaFreeAsync(trial, s);
         if (f1) cudaFreeAsync(f1, s);
         if (qp_iters) cudaFreeAsync(qp_iters, s);
-        A = part = fgh = dir = trial = f1 = nullptr;
+        if (rr) cudaFreeAsync(rr, s);
+        if (sq) cudaFreeAsync(sq, s);
+        A = part = fgh = dir = trial = f1 = rr = sq = nullptr;
         qp_iters = nullptr;
     }
 };
@@ -496,6 +542,10 @@ int sm_count(int dev)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     return sms;
 }
+
+// blocks of the spectrum-model kernels: four per SM (k_ie_gh holds 62
+// registers x 256 threads and 34 KB of shared memory, so four fit)
+int spectrum_grid(int dev) { return 4 * sm_count(dev); }
 
 template <class T>
 int fetch(T *h, const T *d, size_t n, cudaStream_t s)
@@ -522,7 +572,8 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
     double fcur = 0.0;
     int done = 0;
     for (int it = 0; it < newton_steps && !st; ++it) {
-        k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, 1, m->noise, ws.part);
+        k_ie_rays<<<ws.blocks, 256, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, m->noise, w, ws.rr, ws.sq, ws.part);
+        k_ie_gh<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, nr, J, ws.rr, ws.sq, w, ws.part);
         k_ie_sum<<<1, 256, 0, s>>>(ws.part, ws.blocks, w, w, ws.fgh);
         k_ie_qp<<<1, 32, 0, s>>>(ws.fgh, d_Ie, J, ws.dir, ws.qp_iters);
         if ((st = cuda_error(cudaGetLastError(), "spectrum Newton"))) break;
@@ -531,7 +582,7 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
         bool accepted = false, converged = false;
         for (int ls = 0; ls < 40; ++ls, step *= 0.8) {
             k_ie_trial<<<1, 32, 0, s>>>(d_Ie, ws.dir, ws.fgh, J, step, ws.trial);
-            k_ie_eval<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, 0, m->noise, ws.part);
+            k_ie_f<<<ws.blocks, 256, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, m->noise, w, ws.part);
             k_ie_sum<<<1, 256, 0, s>>>(ws.part, ws.blocks, w, 1, ws.f1);
             double fn = 0.0, gd = 0.0;
             if ((st = cuda_error(cudaMemcpyAsync(&fn, ws.f1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
@@ -566,7 +617,7 @@ extern "C" int ctprj_bhc_spectrum_step(ctprj_bhc *m, const float *d_imea, double
     if (newton_steps < 1) return set_error(CTPRJ_EINVAL, "newton_steps must be >= 1");
     cudaStream_t s = (cudaStream_t)stream;
     SpectrumWs ws;
-    int st = ws.alloc(m->J, (long long)m->plan->g.np * m->plan->g.W, 2 * sm_count(m->plan->device), s);
+    int st = ws.alloc(m->J, (long long)m->plan->g.np * m->plan->g.W, spectrum_grid(m->plan->device), s);
     if (st) return st;
     st = spectrum_steps(m, d_imea, d_Ie, newton_steps, f_out, ws, nullptr, s);
     ws.release(s);
@@ -699,7 +750,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         (st = cuda_error(cudaMalloc((void **)&b.sum, sizeof(double) * 2), "loop buffers")) ||
         (opts->unfused &&
          (st = cuda_error(cudaMalloc((void **)&b.sino, sizeof(float) * nr), "loop buffers"))) ||
-        (!opts->skip_spectrum && (st = ws.alloc(m->J, nr, pgb, s)))) {
+        (!opts->skip_spectrum && (st = ws.alloc(m->J, nr, spectrum_grid(dev), s)))) {
         b.release();
         return st;
     }
