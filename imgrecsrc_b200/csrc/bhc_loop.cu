@@ -556,7 +556,7 @@ int fetch(T *h, const T *d, size_t n, cudaStream_t s)
 }
 
 // Newton steps on Ie >= 0 over the saved projections m->d_s: model f, g, H
-// (k_ie_eval), the QP direction (k_ie_qp), then a backtracking line search
+// (k_ie_rays, k_ie_gh), the QP direction (k_ie_qp), then a backtracking line search
 // along the feasible direction, step x0.8 (bhc/ActiveSet.m stepShrnk), until
 // f(Ie + a d) <= f + 1e-4 g.(a d).  Stops early when g.d >= -1e-14 |f| (the
 // model predicts no decrease) or no step decreases f.  *f_out: f at the
