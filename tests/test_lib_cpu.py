@@ -77,3 +77,30 @@ def test_gpuprj_before_setup_reports_not_setup():
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT)
     assert r.returncode == 0, r.stderr
     assert int(r.stdout.strip()) == ct._lib.CTPRJ_ENOTSETUP
+
+
+def test_no_cpu_fallback_without_a_device():
+    """Without a CUDA device a valid geometry fails with a CUDA status and a
+    message; nothing computes on the host instead."""
+    code = ("import ctypes, imgrecsrc_b200 as ct; L = ct.lib();"
+            "g = ct.Geometry(64, 91, 30, 60, 1.0, 1.0, 0.0); p = ctypes.c_void_p();"
+            "st = L.ctprj_plan_create(ctypes.byref(g), 0, ctypes.byref(p));"
+            "print(st, bool(p.value), L.ctprj_last_error().decode())")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, env=env)
+    assert r.returncode == 0, r.stderr
+    st, made, msg = r.stdout.strip().split(" ", 2)
+    assert int(st) == ct._lib.CTPRJ_ECUDA and made == "False" and msg
+
+
+def test_python_layer_raises_without_a_device():
+    code = ("import imgrecsrc_b200 as ct\n"
+            "try:\n"
+            "    ct.Projector(ct.Geometry(64, 91, 30, 60, 1.0, 1.0, 0.0), device=0)\n"
+            "    print('made')\n"
+            "except Exception as e:\n"
+            "    print(type(e).__name__)\n")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, env=env)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() != "made"
