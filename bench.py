@@ -260,9 +260,9 @@ def our_arm(args):
     fwd_ms, bwd_ms = statistics.mean(t_fwd), statistics.mean(t_bwd)
     compulsory = 4 * (g.n * g.n + g.np * g.prjWidth)
     if bwd_ms >= fwd_ms:
-        kname, kms, kbytes = "k_backward<fan>", bwd_ms, 4 * nnz_b + compulsory
+        kname, kms, kbytes = "k_backward_tiled<fan>", bwd_ms, 4 * nnz_b + compulsory
     else:
-        kname, kms, kbytes = "k_transpose + k_forward<fan>", fwd_ms, 4 * nnz_f + compulsory + 8 * g.n * g.n
+        kname, kms, kbytes = "k_quad + k_forward<fan>", fwd_ms, 4 * nnz_f + compulsory + 12 * g.n * g.n
     peak, peak_kind = peaks()
     achieved = kbytes / (kms * 1e-3) / 1e9
     traffic = profiled_traffic().get("k_backward_tiled<fan>" if bwd_ms >= fwd_ms else "k_forward<fan>")
