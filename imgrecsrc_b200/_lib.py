@@ -33,7 +33,8 @@ class LoopOpts(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("x_step", ctypes.c_double),
                 ("spectrum_newton_steps", ctypes.c_int), ("skip_spectrum", ctypes.c_int),
                 ("unfused", ctypes.c_int), ("init_step", ctypes.c_int),
-                ("density_method", ctypes.c_int)]
+                ("density_method", ctypes.c_int), ("thresh", ctypes.c_double),
+                ("min_iterations", ctypes.c_int)]
 
 
 class LoopStats(ctypes.Structure):
@@ -42,7 +43,8 @@ class LoopStats(ctypes.Structure):
                 ("final_x_step", ctypes.c_double), ("cost", ctypes.c_double * MAX_TRACE),
                 ("x_step", ctypes.c_double * MAX_TRACE), ("ms", ctypes.c_float),
                 ("ms_spectrum", ctypes.c_float), ("evaluations", ctypes.c_int),
-                ("restarts", ctypes.c_int), ("newton_steps", ctypes.c_int)]
+                ("restarts", ctypes.c_int), ("newton_steps", ctypes.c_int),
+                ("converged", ctypes.c_int), ("x_change", ctypes.c_double * MAX_TRACE)]
 
 
 class Geometry(ctypes.Structure):

@@ -147,18 +147,22 @@ class BHCModel:
         return f.value
 
     def reconstruct(self, x, Ie, imea, iterations, x_step=1.0, spectrum_newton_steps=2,
-                    skip_spectrum=False, unfused=False, init_step="fixed", method="npg", stream=None):
+                    skip_spectrum=False, unfused=False, init_step="fixed", method="npg",
+                    thresh=0.0, min_iterations=0, stream=None):
         """The alternating density / spectrum loop, x and Ie updated in place.
         init_step: 'fixed' (first step x_step), 'bb' or 'hessian' (the
         reference's stepSizeInit rules); method: 'npg' (npg/NPG.m) or 'pg'
-        (npg/PG.m) for the density step.
+        (npg/PG.m) for the density step; thresh > 0 stops early by the
+        reference's rule (relative density change <= thresh in three
+        iterations after the first, more than min_iterations run).
         Returns a dict with the cost after each iteration, the accepted density
         steps and the device time."""
         import torch
         pr = self.projector
         opts = LoopOpts(int(iterations), float(x_step), int(spectrum_newton_steps),
                         1 if skip_spectrum else 0, 1 if unfused else 0,
-                        {"fixed": 0, "bb": 1, "hessian": 2}[init_step], {"npg": 0, "pg": 1}[method])
+                        {"fixed": 0, "bb": 1, "hessian": 2}[init_step], {"npg": 0, "pg": 1}[method],
+                        float(thresh), int(min_iterations))
         st = LoopStats()
         check(lib().ctprj_bhc_reconstruct(self._m, _dev_ptr(x, pr.img_shape, pr.device),
                                           _dptr(Ie, self.J, torch.float64),
@@ -169,4 +173,5 @@ class BHCModel:
                 "cost": list(st.cost[:n]), "x_step": list(st.x_step[:n]),
                 "final_x_step": st.final_x_step, "ms_spectrum": st.ms_spectrum,
                 "evaluations": st.evaluations, "restarts": st.restarts,
-                "newton_steps": st.newton_steps}
+                "newton_steps": st.newton_steps, "converged": bool(st.converged),
+                "x_change": list(st.x_change[:n])}

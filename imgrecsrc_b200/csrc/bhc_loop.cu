@@ -454,6 +454,38 @@ k_vec_dot(const float *__restrict__ a, const float *__restrict__ b, const float 
     }
 }
 
+// per-block partials of |x - xp|^2 and |xp|^2 (the density's relative change)
+__global__ void __launch_bounds__(256)
+k_rel_change(const float *__restrict__ x, const float *__restrict__ xp, long long n, double *__restrict__ part)
+{
+    __shared__ double red[2][8];
+    double dd = 0.0, pp = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double a = (double)x[i], b = (double)xp[i];
+        dd = fma(a - b, a - b, dd);
+        pp = fma(b, b, pp);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        dd += __shfl_down_sync(0xffffffffu, dd, o);
+        pp += __shfl_down_sync(0xffffffffu, pp, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = dd;
+        red[1][threadIdx.x >> 5] = pp;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a0 += red[0][w];
+            a1 += red[1][w];
+        }
+        part[2 * blockIdx.x] = a0;
+        part[2 * blockIdx.x + 1] = a1;
+    }
+}
+
 // out = x + alpha g
 __global__ void __launch_bounds__(256)
 k_axpy(const float *__restrict__ x, const float *__restrict__ g, float alpha, long long n, float *__restrict__ out)
@@ -758,7 +790,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     const bool pg = opts->density_method == CTPRJ_DENSITY_PG;
     double t = 1.0 / (opts->x_step > 0 ? opts->x_step : 1.0);   // inverse step size
     double theta = 0.0, cost = INFINITY;
-    int p = 0, cumu = 0, cumu_tol = 4, evals = 0, restarts = 0, newton_done = 0;
+    int p = 0, cumu = 0, cumu_tol = 4, evals = 0, restarts = 0, newton_done = 0, conv = 0, converged = 0;
     const int pre_steps = 10;
     const double shrink = 0.5;
     float ms_spec = 0.0f;
@@ -871,6 +903,19 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         }
         if (stats && it < CTPRJ_BHC_LOOP_MAX_TRACE) stats->cost[it] = cost;
         done = it + 1;
+        // relativeDif(x_new, x) of the reference loop; xprev holds this
+        // iteration's starting density
+        k_rel_change<<<pgb, 256, 0, s>>>(d_x, b.xprev, npx, b.part);
+        k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 2, b.sum);
+        double dp[2];
+        if ((st = cuda_error(cudaGetLastError(), "relative change")) || (st = fetch(dp, b.sum, 2, s))) break;
+        const double change = sqrt(dp[0]) / fmax(sqrt(dp[1]), 1e-10);
+        if (stats && it < CTPRJ_BHC_LOOP_MAX_TRACE) stats->x_change[it] = change;
+        if (opts->thresh > 0.0 && it > 0 && change <= opts->thresh) ++conv;
+        if (conv > 2 && done > opts->min_iterations) {
+            converged = 1;
+            break;
+        }
     }
     cudaEventRecord(e1, s);
     cudaEventSynchronize(e1);
@@ -889,6 +934,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         stats->evaluations = evals;
         stats->restarts = restarts;
         stats->newton_steps = newton_done;
+        stats->converged = converged;
     }
     ws.release(s);
     cudaStreamSynchronize(s);

@@ -45,6 +45,12 @@ typedef struct {
                                    plus a separate spectrum-terms kernel (comparison) */
     int init_step;              /* CTPRJ_STEP_*: how the first 1/t is chosen */
     int density_method;         /* CTPRJ_DENSITY_* */
+    double thresh;              /* > 0: stop once the density's relative change
+                                   |x_new - x| / |x| has been <= thresh in three
+                                   iterations after the first, and more than
+                                   min_iterations have run (bhc/beamhardenSpline.m:
+                                   563-566); <= 0: run `iterations` */
+    int min_iterations;
 } ctprj_bhc_loop_opts;
 
 typedef struct {
@@ -60,6 +66,8 @@ typedef struct {
                                                  forward projection) */
     int restarts;                             /* momentum restarts */
     int newton_steps;                         /* accepted spectrum Newton steps */
+    int converged;                            /* 1: stopped by the thresh rule */
+    double x_change[CTPRJ_BHC_LOOP_MAX_TRACE];  /* |x_new - x| / |x| of each iteration */
 } ctprj_bhc_loop_stats;
 
 /* Spectrum update on the projections of the last forward saved by the model

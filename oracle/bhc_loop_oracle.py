@@ -16,7 +16,8 @@ oracle.backward):
   way), then backtracking by 0.8 (bhc/ActiveSet.m stepShrnk) to
   f <= f0 + 1e-4 g.d;
 * alternation as bhc/beamhardenSpline.m:380-470: one density step, then the
-  spectrum step, whose f becomes the cost the next density step compares to.
+  spectrum step, whose f becomes the cost the next density step compares to;
+  optionally the stopping rule of :563-566 on the relative density change.
 """
 import math
 
@@ -171,7 +172,8 @@ class _Density:
 
 
 def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, newton_steps=2,
-                method="npg", init_step="fixed", noise="poisson", skip_spectrum=False):
+                method="npg", init_step="fixed", noise="poisson", skip_spectrum=False, thresh=0.0,
+                min_iterations=0):
     """The alternating loop; forward(x) -> sinogram and backward(sino) -> image
     are FP64 projector callables.  Returns (x, Ie, stats) with stats holding
     the cost and accepted density step of every iteration."""
@@ -198,8 +200,9 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
     pg = method == "pg"
     theta, cost, p, cumu, cumu_tol = 0.0, math.inf, 0, 0, 4
     xprev = x.copy()
-    costs, steps = [], []
-    for _ in range(iterations):
+    costs, steps, changes = [], [], []
+    conv, converged = 0, False
+    for it in range(iterations):
         moved = False
         for pass_ in range(3):
             p += 1
@@ -255,4 +258,13 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
             A, _, _ = BO.b1_basis(k, dens.s(x), derivs=0)
             Ie, cost, _ = spectrum_steps(A, imea, Ie, newton_steps, noise)
         costs.append(cost)
-    return x, Ie, {"cost": costs, "x_step": steps, "final_x_step": 1.0 / t}
+        # relativeDif(x_new, x) and the stopping rule of bhc/beamhardenSpline.m:563-566
+        change = float(np.linalg.norm(x - xprev)) / max(float(np.linalg.norm(xprev)), 1e-10)
+        changes.append(change)
+        if thresh > 0 and it > 0 and change <= thresh:
+            conv += 1
+        if conv > 2 and it + 1 > min_iterations:
+            converged = True
+            break
+    return x, Ie, {"cost": costs, "x_step": steps, "final_x_step": 1.0 / t, "x_change": changes,
+                   "converged": converged}

@@ -172,3 +172,27 @@ def test_loop_tracks_the_fp64_oracle_loop(method, noise):
     assert ec < 1e-4
     assert ex < 1e-4
     assert eI < 1e-3
+
+
+def test_stopping_rule_matches_the_fp64_oracle_loop():
+    """The reference's stopping rule (relative density change <= thresh in
+    three iterations after the first, more than min_iterations run) stops the
+    GPU loop and the FP64 loop at the same iteration, with the same changes."""
+    from oracle import bhc_loop_oracle as LO
+    g, Ts, x_true, k, I_true, m = setup_problem(J=20, seed=4)
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    dx = torch.full((g.n, g.n), 1.0, device="cuda")
+    dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
+    dm = torch.from_numpy(m).cuda()
+    st = model.reconstruct(dx, dI, dm, iterations=60, x_step=1e-3, method="pg", thresh=2e-2, min_iterations=5)
+    fw = lambda x: oracle.forward(g, x)
+    bw = lambda y: oracle.backward(g, y.reshape(g.np, g.prjWidth))
+    xo, Io, so = LO.reconstruct(fw, bw, k, Ts, np.ones((g.n, g.n)), np.full(20, 1.0 / 20),
+                                m.astype(np.float64), 60, x_step=1e-3, method="pg", thresh=2e-2,
+                                min_iterations=5)
+    print("stopping rule: gpu %d iterations (converged %s), oracle %d (converged %s)" % (
+        st["iterations"], st["converged"], len(so["cost"]), so["converged"]))
+    assert st["converged"] and so["converged"]
+    assert st["iterations"] == len(so["cost"]) < 60
+    assert np.allclose(st["x_change"], so["x_change"], rtol=1e-4, atol=0)
