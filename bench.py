@@ -514,7 +514,7 @@ def batch_leg(ct, flush, stream, steps):
         out[name + "_ms"] = ms
         out[name + "_gray_px_per_s"] = updates / (ms * 1e-3) / 1e9
     out["speedup"] = out["per_slice_ms"] / out["batched_ms"]
-    out["batched_launches_per_step"] = 5   # 2 counter resets, transpose, forward, backward
+    out["batched_launches_per_step"] = 5   # 2 counter resets, quad image, forward, backward
     b.close()
     for p in projs:
         p.close()

@@ -2,7 +2,7 @@
 // captured in CUDA graphs, with launch shapes chosen by a tuner.
 //
 // Each slice has its own plan (tables, scratch).  A batched forward is one
-// batched transpose plus one persistent forward kernel over the blocks of all
+// batched quad-image pass plus one persistent forward kernel over the blocks of all
 // slices; a batched backprojection is one persistent kernel over the tiles of
 // all slices (projector.cu, k_*_batch).  Results are identical to the slices'
 // own ctprj_forward / ctprj_backward: the block bodies are the same.

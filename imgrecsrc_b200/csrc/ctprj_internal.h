@@ -109,7 +109,7 @@ struct BatchArgs {
     const int *order;
     const long long *prefix;       // forward blocks or backward tiles
     long long total;
-    const long long *tprefix;      // transpose tiles (natural order)
+    const long long *tprefix;      // quad-image tiles (natural order)
     long long ttotal;
     unsigned long long *counter;   // work counter, zero before each launch
 };

@@ -10,9 +10,9 @@
 //
 //  forward   one thread per base ray (view b <= prjFull/8, detector k), marching
 //            down the image rows (ray-driven, prj/cpuPrj.c:319-616).  The eight
-//            mirrored pixels of a row come from four contiguous row segments:
-//            rows y and -y of the image and of its transpose, which the plan
-//            keeps in scratch so that every gather is coalesced along x.
+//            mirrored pixels of a pixel come from the plan's quad image (two
+//            float4 per pixel, built at the start of each call), so that every
+//            gather is a 16-byte load coalesced along x.
 //  backward  one thread per octant pixel 0 <= y <= x (pixel-driven,
 //            prj/cpuPrj.c:46-317), looping over the base views and the
 //            detectors under the pixel's shadow; each thread owns its eight
@@ -22,6 +22,7 @@
 // FP64 before rounding (x cos R + y sin R - offset cancels to O(1) from terms
 // of O(n)); that keeps the projections within 1e-7..1e-6 of the FP64 oracle,
 // where the reference's own FP32 build is 1.5e-5 off on signed inputs.
+// The footprint itself is branch-free (footprint.cuh).
 #include <cstdio>
 #include <type_traits>
 

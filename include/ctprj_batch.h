@@ -5,7 +5,7 @@
  * per gpuPrj() call (prj/gpuPrj.cu:887-1047) and reconfigures with setup()
  * between geometries; a batch replaces that loop.  Each slice keeps the exact
  * semantics of ctprj_forward / ctprj_backward for its geometry (results are
- * identical); the whole batch runs as one batched transpose plus one persistent
+ * identical); the whole batch runs as one batched quad-image pass plus one persistent
  * forward kernel, or one persistent backprojection kernel, and can be captured
  * in CUDA graphs.  Launch shapes are chosen by ctprj_batch_autotune.
  */
