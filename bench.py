@@ -41,6 +41,8 @@ L2_FLUSH_BYTES = 512 << 20   # > 126 MB L2
 # phantom (0 / 2.7 / 7.8 g/cm^3), J = 30 b1 coefficients on kappa log-spaced over
 # [1e-2, 1e2] cm^2/g, Poisson counts at I0 = 1e5 per ray, 2 cm field of view
 BHC = dict(J=30, I0=1e5, fov_cm=2.0)
+# the double-precision masked parallel operator (mParPrj) measured beside
+PARPRJ = dict(n=512, prjWidth=727, np=360)
 # the polychromatic model's own configuration: fan 1024^2, 720 views over
 # [0, 2 pi), 1024 detectors, source 2048 px from the isocentre
 BHC_WORKLOAD = dict(n=1024, prjWidth=1024, np=720, prjFull=720, dSize=1.0, effectiveRate=1.0, d=2048.0)
@@ -190,6 +192,27 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def cpu_parprj_run():
+    """The reference's own prj/parPrj.c (oracle/_ref) on the host cores, on the
+    masked parallel operator workload of extras_leg: (forward s, backward s)."""
+    import numpy as np
+
+    from oracle import ref
+    if not ref.available("libref_parprj"):
+        return None
+    n, W, nang = PARPRJ["n"], PARPRJ["prjWidth"], PARPRJ["np"]
+    r = np.arange(n) - (n - 1) / 2
+    mask = np.flatnonzero(((r[:, None] ** 2 + r[None, :] ** 2) <= (0.48 * n) ** 2).ravel(order="F"))
+    conf = dict(bw=1.0, nc=n, nr=n, prjWidth=W, theta=np.arange(nang) * 180.0 / nang)
+    x = np.random.default_rng(5).random(mask.size)
+    t0 = time.perf_counter()
+    y = ref.par_forward(x, mask, conf)
+    t1 = time.perf_counter()
+    ref.par_backward(y, mask, conf)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1
+
+
 def our_arm(args):
     import numpy as np
     import torch
@@ -277,6 +300,7 @@ def our_arm(args):
                                     "fan 2048^2, 1440 views, 2048 bins, d=8192 px")}
     pr3.close()
     batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
+    extras_line = extras_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
     loop_line = None
     if args.loop_iters > 0:
         if args.loop_geometry == "1024":
@@ -332,10 +356,16 @@ def our_arm(args):
         "bhc": bhc_line,
         "batch": batch_line,
         "bhc_loop": loop_line,
+        "extras": extras_line,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         v, t, info = cpu_reference_run(1, 0)
         line["cpu_baseline"] = dict(value=v, unit="Gray-px/s", **info)
+        par = cpu_parprj_run()
+        if par:
+            line["cpu_baseline"]["parprj"] = {"kind": "reference", "forward_ms": par[0] * 1e3,
+                                              "backward_ms": par[1] * 1e3,
+                                              "threads": 32}   # parPrj.c runs 32 pthreads
     if pg:
         pg.barrier()
         pg.destroy_process_group()
@@ -518,6 +548,63 @@ def batch_leg(ct, flush, stream, steps):
     b.close()
     for p in projs:
         p.close()
+    return out
+
+
+def extras_leg(ct, g, pr, flush, stream, steps):
+    """FBP on the headline geometry, and the double-precision masked parallel
+    operator of mParPrj (prj/parPrj.c) on device buffers: 512^2 image, a disc
+    mask, 360 angles over [0, 180) degrees, 727 detectors."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ms = 0.0
+        for _ in range(steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        return ms / steps
+
+    out = {}
+    y = torch.randn(g.np, g.prjWidth, device="cuda", generator=torch.Generator(device="cuda").manual_seed(5))
+    img = torch.empty(g.n, g.n, device="cuda")
+    out["fbp_ms"] = timed(lambda: pr.fbp(y, out=img))
+    n, W, nang = PARPRJ["n"], PARPRJ["prjWidth"], PARPRJ["np"]
+    r = np.arange(n) - (n - 1) / 2
+    mask = np.flatnonzero(((r[:, None] ** 2 + r[None, :] ** 2) <= (0.48 * n) ** 2).ravel(order="F"))
+    theta = np.ascontiguousarray(np.arange(nang) * 180.0 / nang)
+    conf = ct._lib.ParDevConf(1.0, n, n, nang, W)
+    d_mask = torch.from_numpy(mask.astype(np.float64)).cuda()
+    d_x = torch.rand(mask.size, dtype=torch.float64, device="cuda")
+    d_y = torch.zeros(nang * W, dtype=torch.float64, device="cuda")
+    d_b = torch.zeros(mask.size, dtype=torch.float64, device="cuda")
+    L = ct.lib()
+    hs = ctypes.c_void_p(stream.cuda_stream)
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def fwd():
+        d_y.zero_()
+        ct.check(L.ctprj_par_forward(ctypes.byref(conf), theta.ctypes.data, vp(d_mask), mask.size,
+                                     vp(d_x), vp(d_y), hs))
+
+    def bwd():
+        d_b.zero_()
+        ct.check(L.ctprj_par_backward(ctypes.byref(conf), theta.ctypes.data, vp(d_mask), mask.size,
+                                      vp(d_y), vp(d_b), hs))
+    out["parprj"] = {"workload": "FP64 masked parallel operator (mParPrj): %d^2 image, disc mask of %d "
+                                 "pixels, %d angles over [0,180) deg, %d detectors" % (n, mask.size, nang, W),
+                     "forward_ms": timed(fwd), "backward_ms": timed(bwd)}
     return out
 
 

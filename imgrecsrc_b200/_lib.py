@@ -47,6 +47,12 @@ class LoopStats(ctypes.Structure):
                 ("converged", ctypes.c_int), ("x_change", ctypes.c_double * MAX_TRACE)]
 
 
+class ParDevConf(ctypes.Structure):
+    """ctprj_par_conf of include/parprj.h (device-pointer form)."""
+    _fields_ = [("bw", ctypes.c_double), ("nc", ctypes.c_int), ("nr", ctypes.c_int),
+                ("np", ctypes.c_int), ("prjWidth", ctypes.c_int)]
+
+
 class Geometry(ctypes.Structure):
     """struct ctprj_geometry -- the reference's projector configuration
     (prj/prj.h:42-57): n, prjWidth, np, prjFull, dSize, effectiveRate, d."""
@@ -105,6 +111,8 @@ def lib():
         "ctprj_bhc_set_noise": ([VP, ctypes.c_int], ctypes.c_int),
         "ctprj_bhc_hessian": ([VP, VP, VP, VP, VP, VP, VP], ctypes.c_int),
         "parPrjConf": ([VP, VP, VP, ctypes.POINTER(ParConf), ctypes.c_size_t], ctypes.c_int),
+        "ctprj_par_forward": ([ctypes.POINTER(ParDevConf), VP, VP, ctypes.c_longlong, VP, VP, VP], ctypes.c_int),
+        "ctprj_par_backward": ([ctypes.POINTER(ParDevConf), VP, VP, ctypes.c_longlong, VP, VP, VP], ctypes.c_int),
         "parPrjThread": ([], ctypes.c_int),
         "parPrjRun": ([], ctypes.c_int),
         "ctprj_batch_create": ([GP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(VP)], ctypes.c_int),
