@@ -9,8 +9,8 @@
 // wrap-around never reaches the padding, so the filter is the symmetric
 // Toeplitz product out[m] = sum_n x[n] h[|m - n|].  The plan derives h once, in
 // FP64 on the host, from the reference's own taps (its ramp values are formed in
-// float arithmetic, prj/utils.h:117-121); the device applies it directly, one
-// block per view row with the row and the taps staged in shared memory.
+// float arithmetic, prj/utils.h:117-121); the device applies it directly as a
+// register-tiled product (k_fbp_filter).
 #include <cmath>
 #include <vector>
 
@@ -18,8 +18,6 @@
 
 namespace ctprj {
 
-constexpr int kFiltThreads = 256;
-constexpr int kFiltChunk = 4096;   // row / tap elements staged per pass
 
 // taps h[0..W-1] of the reference's ramp filter for a row of W detectors
 static std::vector<double> ramp_taps(int W)
@@ -55,39 +53,79 @@ static std::vector<double> ramp_taps(int W)
     return h;
 }
 
-__global__ void __launch_bounds__(kFiltThreads)
+// The filter as a register-tiled Toeplitz product.  A block of kFT threads
+// owns kFO = kFT * kFR consecutive outputs of kFV view rows; thread t the kFR
+// consecutive outputs mt = m0 + kFR t .. mt + kFR - 1 of every row, in
+// kFV * kFR accumulators.  Inputs go through shared memory in chunks of kFN,
+// with the taps of the chunk's lag window; for input n the thread needs the
+// kFR taps h[|mt + r - n|], r < kFR, which slide by one element per input, so
+// it keeps them in registers and loads one new tap per input: kFV + 1 shared
+// loads (kFV of them broadcasts) per kFV * kFR FMAs.  The lag window is stored
+// with one pad per 32 taps, so that lanes kFR apart read distinct banks.
+constexpr int kFT = 128, kFR = 8, kFV = 4, kFN = 256;
+constexpr int kFO = kFT * kFR;
+constexpr int kFH = kFO + kFN;   // lag window length (one spare)
+
+__device__ __forceinline__ int skew(int i) { return i + (i >> 5); }
+
+__global__ void __launch_bounds__(kFT)
 k_fbp_filter(const float *__restrict__ sino, float *__restrict__ out, const float *__restrict__ taps,
              const float *__restrict__ colw, int W, int np)
 {
-    __shared__ float xs[kFiltChunk];
-    __shared__ float hs[2 * kFiltChunk];
-    const int v = blockIdx.y;
-    if (v >= np) return;
-    const float *row = sino + (size_t)v * W;
-    const int m0 = blockIdx.x * kFiltThreads;
-    const int m = m0 + threadIdx.x;
-    float acc = 0.0f;
-    // outputs m0..m0+255 need taps |m - n| for n in the staged input chunk
-    for (int n0 = 0; n0 < W; n0 += kFiltChunk) {
-        const int nlen = min(kFiltChunk, W - n0);
+    __shared__ float xs[kFV][kFN];
+    __shared__ float hs[kFH + kFH / 32 + 1];
+    const int m0 = blockIdx.x * kFO, v0 = blockIdx.y * kFV;
+    const int lane0 = threadIdx.x * kFR;   // mt - m0
+    float acc[kFV][kFR];
+#pragma unroll
+    for (int v = 0; v < kFV; ++v)
+#pragma unroll
+        for (int r = 0; r < kFR; ++r) acc[v][r] = 0.0f;
+    for (int n0 = 0; n0 < W; n0 += kFN) {
         __syncthreads();
-        for (int i = threadIdx.x; i < nlen; i += kFiltThreads)
-            xs[i] = row[n0 + i] * (colw ? colw[n0 + i] : 1.0f);
-        // tap window: lags from (m0 - (n0 + nlen - 1)) to (m0 + 255 - n0)
-        const int lag_lo = m0 - (n0 + nlen - 1);
-        const int nl = nlen + kFiltThreads - 1;
-        for (int i = threadIdx.x; i < nl; i += kFiltThreads) {
-            const int lag = abs(lag_lo + i);
-            hs[i] = lag < W ? taps[lag] : 0.0f;
+        for (int e = threadIdx.x; e < kFV * kFN; e += kFT) {
+            const int v = e / kFN, i = e % kFN, n = n0 + i;
+            xs[v][i] = (v0 + v < np && n < W) ? sino[(size_t)(v0 + v) * W + n] * (colw ? colw[n] : 1.0f) : 0.0f;
+        }
+        // hs[j] = h[|lag_lo + j|], lag_lo = m0 - (n0 + kFN - 1): the lag of
+        // output mt + r and input n0 + i is at j = lane0 + r + kFN - 1 - i
+        const int lag_lo = m0 - (n0 + kFN - 1);
+        for (int j = threadIdx.x; j < kFH; j += kFT) {
+            const int lag = abs(lag_lo + j);
+            hs[skew(j)] = lag < W ? taps[lag] : 0.0f;
         }
         __syncthreads();
-        if (m < W) {
-            // lag for input n0 + i is m - n0 - i = (m - m0) + (nlen - 1 - i) + lag_lo
-            const int base = (m - m0) + nlen - 1;
-            for (int i = 0; i < nlen; ++i) acc = fmaf(xs[i], hs[base - i], acc);
+        float w[kFR];
+#pragma unroll
+        for (int r = 0; r < kFR; ++r) w[r] = hs[skew(lane0 + r + kFN - 1)];
+        for (int i0 = 0; i0 < kFN; i0 += kFR) {
+#pragma unroll
+            for (int q = 0; q < kFR; ++q) {
+                const int i = i0 + q;
+                float xv[kFV];
+#pragma unroll
+                for (int v = 0; v < kFV; ++v) xv[v] = xs[v][i];
+#pragma unroll
+                for (int v = 0; v < kFV; ++v)
+#pragma unroll
+                    for (int r = 0; r < kFR; ++r) acc[v][r] = fmaf(xv[v], w[r], acc[v][r]);
+                // the taps of input i + 1 are those of input i shifted by one
+#pragma unroll
+                for (int r = kFR - 1; r > 0; --r) w[r] = w[r - 1];
+                const int jn = lane0 + kFN - 2 - i;
+                w[0] = jn >= 0 ? hs[skew(jn)] : 0.0f;
+            }
         }
     }
-    if (m < W) out[(size_t)v * W + m] = acc;
+#pragma unroll
+    for (int v = 0; v < kFV; ++v) {
+        if (v0 + v >= np) break;
+#pragma unroll
+        for (int r = 0; r < kFR; ++r) {
+            const int m = m0 + lane0 + r;
+            if (m < W) out[(size_t)(v0 + v) * W + m] = acc[v][r];
+        }
+    }
 }
 
 }  // namespace ctprj
@@ -120,9 +158,9 @@ int ctprj_fbp_device(ctprj_plan *plan, const float *d_sino, float *d_img, cudaSt
             return st;
         }
     }
-    dim3 grid((g.W + kFiltThreads - 1) / kFiltThreads, g.np);
-    k_fbp_filter<<<grid, kFiltThreads, 0, s>>>(d_sino, plan->d_fsino, plan->d_ramp,
-                                                g.fan ? plan->d_ramp + g.W : nullptr, g.W, g.np);
+    dim3 grid((g.W + kFO - 1) / kFO, (g.np + kFV - 1) / kFV);
+    k_fbp_filter<<<grid, kFT, 0, s>>>(d_sino, plan->d_fsino, plan->d_ramp,
+                                       g.fan ? plan->d_ramp + g.W : nullptr, g.W, g.np);
     if ((st = cuda_error(cudaGetLastError(), "FBP filter launch"))) return st;
     return launch_backward(plan, plan->d_fsino, d_img, 1, nullptr, s);
 }
