@@ -34,7 +34,8 @@ class LoopOpts(ctypes.Structure):
                 ("spectrum_newton_steps", ctypes.c_int), ("skip_spectrum", ctypes.c_int),
                 ("unfused", ctypes.c_int), ("init_step", ctypes.c_int),
                 ("density_method", ctypes.c_int), ("thresh", ctypes.c_double),
-                ("min_iterations", ctypes.c_int)]
+                ("min_iterations", ctypes.c_int), ("proximal", ctypes.c_int),
+                ("u", ctypes.c_double), ("max_inner", ctypes.c_int)]
 
 
 class LoopStats(ctypes.Structure):
@@ -44,7 +45,9 @@ class LoopStats(ctypes.Structure):
                 ("x_step", ctypes.c_double * MAX_TRACE), ("ms", ctypes.c_float),
                 ("ms_spectrum", ctypes.c_float), ("evaluations", ctypes.c_int),
                 ("restarts", ctypes.c_int), ("newton_steps", ctypes.c_int),
-                ("converged", ctypes.c_int), ("x_change", ctypes.c_double * MAX_TRACE)]
+                ("converged", ctypes.c_int), ("x_change", ctypes.c_double * MAX_TRACE),
+                ("inner_iterations", ctypes.c_int), ("prox_retries", ctypes.c_int),
+                ("penalty", ctypes.c_double)]
 
 
 class ParDevConf(ctypes.Structure):
@@ -131,6 +134,10 @@ def lib():
         "ctprj_masked_forward": ([VP, VP, ctypes.c_longlong, VP, ctypes.c_double, VP, VP], ctypes.c_int),
         "ctprj_masked_backward": ([VP, VP, ctypes.c_longlong, VP, ctypes.c_double, VP, VP], ctypes.c_int),
         "ctprj_masked_fbp": ([VP, VP, ctypes.c_longlong, VP, ctypes.c_double, VP, VP], ctypes.c_int),
+        "ctprj_tv_denoise": ([VP, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                              ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, VP,
+                              ctypes.POINTER(ctypes.c_int), VP], ctypes.c_int),
+        "ctprj_tv_value": ([VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, VP], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

@@ -148,13 +148,17 @@ class BHCModel:
 
     def reconstruct(self, x, Ie, imea, iterations, x_step=1.0, spectrum_newton_steps=2,
                     skip_spectrum=False, unfused=False, init_step="fixed", method="npg",
-                    thresh=0.0, min_iterations=0, stream=None):
+                    thresh=0.0, min_iterations=0, proximal="nonneg", u=0.0, max_inner=100,
+                    stream=None):
         """The alternating density / spectrum loop, x and Ie updated in place.
         init_step: 'fixed' (first step x_step), 'bb' or 'hessian' (the
         reference's stepSizeInit rules); method: 'npg' (npg/NPG.m) or 'pg'
         (npg/PG.m) for the density step; thresh > 0 stops early by the
         reference's rule (relative density change <= thresh in three
-        iterations after the first, more than min_iterations run).
+        iterations after the first, more than min_iterations run);
+        proximal: 'nonneg', 'tviso' or 'tvl1' (the reference's opt.proximal
+        for NPG / PG), the TV maps with penalty weight u and a first inner
+        iteration limit max_inner.
         Returns a dict with the cost after each iteration, the accepted density
         steps and the device time."""
         import torch
@@ -162,7 +166,8 @@ class BHCModel:
         opts = LoopOpts(int(iterations), float(x_step), int(spectrum_newton_steps),
                         1 if skip_spectrum else 0, 1 if unfused else 0,
                         {"fixed": 0, "bb": 1, "hessian": 2}[init_step], {"npg": 0, "pg": 1}[method],
-                        float(thresh), int(min_iterations))
+                        float(thresh), int(min_iterations),
+                        {"nonneg": 0, "tviso": 1, "tvl1": 2}[proximal], float(u), int(max_inner))
         st = LoopStats()
         check(lib().ctprj_bhc_reconstruct(self._m, _dev_ptr(x, pr.img_shape, pr.device),
                                           _dptr(Ie, self.J, torch.float64),
@@ -174,4 +179,5 @@ class BHCModel:
                 "final_x_step": st.final_x_step, "ms_spectrum": st.ms_spectrum,
                 "evaluations": st.evaluations, "restarts": st.restarts,
                 "newton_steps": st.newton_steps, "converged": bool(st.converged),
-                "x_change": list(st.x_change[:n])}
+                "x_change": list(st.x_change[:n]), "inner_iterations": st.inner_iterations,
+                "prox_retries": st.prox_retries, "penalty": st.penalty}

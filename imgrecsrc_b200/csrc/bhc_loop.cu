@@ -408,6 +408,40 @@ k_pg_step(const float *__restrict__ x, const float *__restrict__ g, long long n,
     }
 }
 
+// per-block partials of g . (xn - x) and |xn - x|^2 for a candidate xn that a
+// proximal map other than the projection produced
+__global__ void __launch_bounds__(256)
+k_step_terms(const float *__restrict__ x, const float *__restrict__ g, const float *__restrict__ xn, long long n,
+             double *__restrict__ part)
+{
+    __shared__ double red[2][8];
+    double gd = 0.0, dd = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double d = (double)xn[i] - (double)x[i];
+        gd = fma((double)g[i], d, gd);
+        dd = fma(d, d, dd);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        gd += __shfl_down_sync(0xffffffffu, gd, o);
+        dd += __shfl_down_sync(0xffffffffu, dd, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = gd;
+        red[1][threadIdx.x >> 5] = dd;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a0 = 0.0, a1 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            a0 += red[0][w];
+            a1 += red[1][w];
+        }
+        part[2 * blockIdx.x] = a0;
+        part[2 * blockIdx.x + 1] = a1;
+    }
+}
+
 // Nesterov extrapolation xbar = max(0, x + coef (x - xprev)); per-block
 // partials of sum |xbar - x| (whether the step carries momentum)
 __global__ void __launch_bounds__(256)
@@ -671,10 +705,11 @@ int likelihood(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *
 
 struct LoopBufs {
     float *gx = nullptr, *xn = nullptr, *xbar = nullptr, *xprev = nullptr, *sino = nullptr;
+    float *v = nullptr;   // input of the TV proximal map
     double *f = nullptr, *part = nullptr, *sum = nullptr;
     void release()
     {
-        cudaFree(gx); cudaFree(xn); cudaFree(xbar); cudaFree(xprev); cudaFree(sino);
+        cudaFree(gx); cudaFree(xn); cudaFree(xbar); cudaFree(xprev); cudaFree(sino); cudaFree(v);
         cudaFree(f); cudaFree(part); cudaFree(sum);
     }
 };
@@ -740,8 +775,8 @@ int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, con
 }  // namespace
 
 // The density step follows the reference's NPG class (npg/NPG.m main, with
-// the proximal map reduced to the projection on x >= 0), or its PG class
-// (npg/PG.m: the same without extrapolation and restart):
+// the projection on x >= 0 or the TV denoising of tv.cu as the proximal map),
+// or its PG class (npg/PG.m: the same without extrapolation and restart):
 //   theta' = (1 + sqrt(1 + 4 theta^2)) / 2,  xbar = max(0, x + (theta-1)/theta' (x - xprev));
 //   f, grad at xbar;  candidate xn = max(0, xbar - grad / t), accepted when
 //   f(xn) <= f(xbar) + grad.(xn - xbar) + t/2 |xn - xbar|^2 (utils/Utils.m
@@ -752,8 +787,11 @@ int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, con
 //   if f(xn) exceeds the cost of the previous iteration: restart without
 //   momentum (theta = 1) when xbar != x, else keep x when the majorisation
 //   failed or f(xbar) < f(xn) (PG: keep x when the majorisation failed or the
-//   cost rose).  The reference's further retries with tighter inner ADMM
-//   tolerances do not apply to an exact projection, and its reset of t to the
+//   cost rose).  With a TV map the candidate is TV.denoise(xbar - grad / t,
+//   u / t) to tolerance admmTol * difAlpha, the cost carries u TV, and before
+//   x is kept the step is retried with admmTol / 10 (down to 1e-6) or
+//   maxInnerItr * 10 (up to 1000); those retries cannot change an exact
+//   projection and are not taken for it.  The reference's reset of t to the
 //   Hessian estimate after a failed majorisation is not taken.
 // Then the spectrum step on the accepted density's projections, whose f
 // becomes the cost the next density step compares against
@@ -764,6 +802,11 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
 {
     if (!m || !d_x || !d_Ie || !d_imea || !opts) return set_error(CTPRJ_EINVAL, "NULL argument");
     if (opts->iterations < 0) return set_error(CTPRJ_EINVAL, "negative iteration count");
+    const int prox = opts->proximal;
+    if (prox != CTPRJ_PROX_NONNEG && prox != CTPRJ_PROX_TV_ISO && prox != CTPRJ_PROX_TV_L1)
+        return set_error(CTPRJ_EINVAL, "unknown proximal map %d", prox);
+    const bool tv = prox != CTPRJ_PROX_NONNEG;
+    if (tv && !(opts->u > 0.0)) return set_error(CTPRJ_EINVAL, "the TV proximal maps need u > 0");
     PlanDevice pd(m->plan->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long npx = (long long)m->plan->g.n * m->plan->g.n;
@@ -772,6 +815,8 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     const int pgb = 2 * sm_count(dev);
     LoopBufs b;
     SpectrumWs ws;
+    TvWorkspace tvw;
+    const int n = m->plan->g.n;
     int st;
     if ((st = cuda_error(cudaMalloc((void **)&b.gx, sizeof(float) * npx), "loop buffers")) ||
         (st = cuda_error(cudaMalloc((void **)&b.xn, sizeof(float) * npx), "loop buffers")) ||
@@ -779,10 +824,14 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         (st = cuda_error(cudaMalloc((void **)&b.xprev, sizeof(float) * npx), "loop buffers")) ||
         (st = cuda_error(cudaMalloc((void **)&b.f, sizeof(double) * 2), "loop buffers")) ||
         (st = cuda_error(cudaMalloc((void **)&b.part, sizeof(double) * 2 * pgb), "loop buffers")) ||
-        (st = cuda_error(cudaMalloc((void **)&b.sum, sizeof(double) * 2), "loop buffers")) ||
+        (st = cuda_error(cudaMalloc((void **)&b.sum, sizeof(double) * 4), "loop buffers")) ||
+        (tv && (st = cuda_error(cudaMalloc((void **)&b.v, sizeof(float) * npx), "loop buffers"))) ||
+        (tv && (st = tvw.alloc(n, n, s))) ||
         (opts->unfused &&
          (st = cuda_error(cudaMalloc((void **)&b.sino, sizeof(float) * nr), "loop buffers"))) ||
         (!opts->skip_spectrum && (st = ws.alloc(m->J, nr, spectrum_grid(dev), s)))) {
+        tvw.release(s);
+        cudaStreamSynchronize(s);
         b.release();
         return st;
     }
@@ -793,6 +842,30 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     int p = 0, cumu = 0, cumu_tol = 4, evals = 0, restarts = 0, newton_done = 0, conv = 0, converged = 0;
     const int pre_steps = 10;
     const double shrink = 0.5;
+    // the TV proximal map's state (npg/NPG.m:11,23-24 and Methods.m difAlpha = 1)
+    const bool iso = prox == CTPRJ_PROX_TV_ISO;
+    const int max_pass = tv ? 12 : 3;
+    double admm_tol = 1e-2, dif_alpha = 1.0, pen = 0.0;
+    int max_inner = opts->max_inner > 0 ? opts->max_inner : 100, inner = 0, inner_total = 0, retries = 0;
+    auto penalty_of = [&](const float *v, double *out) -> int {   // u TV(v)
+        double tvv = 0.0;
+        int e = tv_value(tvw, v, n, n, iso, b.sum + 3, s);
+        if (!e) e = fetch(&tvv, b.sum + 3, 1, s);
+        *out = opts->u * tvv;
+        return e;
+    };
+    // a rejected TV step is retried with a tighter inner tolerance or, when the
+    // inner iteration ran out, more inner iterations (npg/NPG.m:117-128)
+    auto retry = [&]() -> bool {
+        if (inner < max_inner && admm_tol > 1e-6)
+            admm_tol /= 10.0;
+        else if (inner >= max_inner && max_inner < 1000)
+            max_inner *= 10;
+        else
+            return false;
+        ++retries;
+        return true;
+    };
     float ms_spec = 0.0f;
     cudaEvent_t e0, e1, es0, es1;
     cudaEventCreate(&e0);
@@ -807,9 +880,10 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     }
     int done = 0;
     for (int it = 0; it < opts->iterations && !st; ++it) {
-        double nc = 0.0;
+        double nc = 0.0, obj = 0.0;
         bool moved = false, state_at_x = false;
-        for (int pass = 0; pass < 3 && !st; ++pass) {
+        for (int pass = 0; pass < max_pass && !st; ++pass) {
+            const bool last = pass == max_pass - 1;
             ++p;
             const double theta1 = (1.0 + sqrt(1.0 + 4.0 * theta * theta)) / 2.0;
             const float coef = pg ? 0.0f : (float)((theta - 1.0) / theta1);
@@ -832,7 +906,17 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             }
             while (true) {
                 ++ppp;
-                k_pg_step<<<pgb, 256, 0, s>>>(b.xbar, b.gx, npx, (float)(1.0 / t), b.xn, b.part);
+                if (tv) {   // xn = TV.denoise(xbar - g / t, u / t, admmTol difAlpha, maxInnerItr)
+                    k_axpy<<<pgb, 256, 0, s>>>(b.xbar, b.gx, (float)(-1.0 / t), npx, b.v);
+                    if ((st = cuda_error(cudaGetLastError(), "density step")) ||
+                        (st = tv_denoise(tvw, b.v, n, n, opts->u / t, 0.0, INFINITY, iso, max_inner,
+                                         admm_tol * dif_alpha, b.xn, &inner, s)))
+                        break;
+                    inner_total += inner;
+                    k_step_terms<<<pgb, 256, 0, s>>>(b.xbar, b.gx, b.xn, npx, b.part);
+                } else {
+                    k_pg_step<<<pgb, 256, 0, s>>>(b.xbar, b.gx, npx, (float)(1.0 / t), b.xn, b.part);
+                }
                 k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 2, b.sum);
                 double gd_dd[2];
                 if ((st = cuda_error(cudaGetLastError(), "density step")) ||
@@ -861,28 +945,46 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                 }
             }
             if (st) break;
+            if (tv && (st = penalty_of(b.xn, &pen))) break;
+            obj = nc + pen;
             moved = true;
             if (pg) {
-                if (!good_mm || nc > cost) moved = false;   // npg/PG.m: force convergence
-            } else if (nc > cost) {
-                if (good_mm && mom != 0.0 && pass < 2) {   // restart without momentum
+                if (!good_mm || obj > cost) {
+                    if (tv && !last && retry()) continue;
+                    moved = false;                          // npg/PG.m: force convergence
+                }
+            } else if (obj > cost) {
+                if (good_mm && mom != 0.0 && !last) {      // restart without momentum
                     theta = 1.0;
                     ++restarts;
                     continue;
                 }
-                if (!good_mm || f0 < nc) moved = false;     // npg/NPG.m: force convergence
+                double pen_bar = 0.0;
+                if (tv && good_mm && (st = penalty_of(b.xbar, &pen_bar))) break;
+                if (!good_mm || f0 + pen_bar < obj) {
+                    if (!good_mm) theta = 1.0;              // NPG's reset() (its t reset is not taken)
+                    if (tv && !last && retry()) continue;
+                    moved = false;                          // npg/NPG.m: force convergence
+                }
             }
-            if (!moved) nc = cost;   // keep x
+            if (!moved) obj = cost;   // keep x
             theta = theta1;
             st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "accept");
             if (!st && moved)
                 st = cuda_error(cudaMemcpyAsync(d_x, b.xn, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "accept");
+            if (!st && tv) {   // difAlpha = relativeDif(x, x_new), the next inner tolerance's scale
+                k_rel_change<<<pgb, 256, 0, s>>>(b.xprev, d_x, npx, b.part);
+                k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 2, b.sum);
+                double dq[2];
+                if (!(st = cuda_error(cudaGetLastError(), "relative change")) && !(st = fetch(dq, b.sum, 2, s)))
+                    dif_alpha = sqrt(dq[0]) / fmax(sqrt(dq[1]), 1e-10);
+            }
             state_at_x = moved;   // the last likelihood evaluated (and saved) was at xn
             cumu = ppp == 1 ? cumu + 1 : 0;
             break;
         }
         if (st) break;
-        cost = nc;
+        cost = obj;
         if (stats && it < CTPRJ_BHC_LOOP_MAX_TRACE) stats->x_step[it] = moved ? 1.0 / t : 0.0;
         if (!opts->skip_spectrum) {
             cudaEventRecord(es0, s);
@@ -899,7 +1001,9 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             float ms = 0.0f;
             cudaEventElapsedTime(&ms, es0, es1);
             ms_spec += ms;
-            cost = fs;
+            // alphaStep.cost = IeStep.cost + u fVal(3) (bhc/beamhardenSpline.m:460): the
+            // penalty of the last density candidate, also when it was not accepted
+            cost = fs + pen;
         }
         if (stats && it < CTPRJ_BHC_LOOP_MAX_TRACE) stats->cost[it] = cost;
         done = it + 1;
@@ -935,8 +1039,12 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         stats->restarts = restarts;
         stats->newton_steps = newton_done;
         stats->converged = converged;
+        stats->inner_iterations = inner_total;
+        stats->prox_retries = retries;
+        stats->penalty = pen;
     }
     ws.release(s);
+    tvw.release(s);
     cudaStreamSynchronize(s);
     b.release();
     return st;

@@ -202,6 +202,22 @@ struct PlanDevice {
 int set_error(int status, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
 
+// buffers of the TV proximal map (tv.cu): D, P1, P2 double-buffered, R1, R2
+// (8 images), per-block FP64 partials and the device-side iteration state
+struct TvWorkspace {
+    float *buf = nullptr;
+    double *part = nullptr;
+    void *state = nullptr;
+    int rows = 0, cols = 0, blocks = 0;
+    int alloc(int m, int n, cudaStream_t s);
+    void release(cudaStream_t s);
+};
+// D = argmin ||X - xobs||^2 + 2 lambda TV(X), lb <= X <= ub (tv.cu)
+int tv_denoise(TvWorkspace &ws, const float *xobs, int m, int n, double lambda, double lb, double ub,
+               int iso, int max_iter, double eps, float *out, int *iterations, cudaStream_t s);
+// *d_out = TV(x) in FP64 (device)
+int tv_value(TvWorkspace &ws, const float *x, int m, int n, int iso, double *d_out, cudaStream_t s);
+
 // launchers (projector.cu)
 // the quad image of the forward pass (projector.cu): (half + 1) rows of
 // 2 half + 1 float4, built in 32 x 32 tiles

@@ -3,8 +3,8 @@
  *
  * Counterpart of the reference's BHC driver loop (bhc/beamhardenSpline.m:
  * 340-570): one density step on the likelihood (the reference's NPG class,
- * npg/NPG.m, or its PG class, npg/PG.m, with the non-negativity projection as
- * the proximal map),
+ * npg/NPG.m, or its PG class, npg/PG.m, with the non-negativity projection or
+ * the TV denoising of include/ctprj_tv.h as the proximal map),
  * then a non-negative spectrum step, repeated.  Built on the model of
  * include/ctprj.h (ctprj_bhc_*): every likelihood and gradient of the density
  * step comes from the fused forward projection and its adjoint; the spectrum
@@ -35,6 +35,11 @@ extern "C" {
                                  the reference's default, bhc/beamhardenSpline.m:37) */
 #define CTPRJ_DENSITY_PG 1    /* proximal (projected) gradient (npg/PG.m) */
 
+/* proximal map of the density step (opt.proximal, bhc/beamhardenSpline.m:199-223) */
+#define CTPRJ_PROX_NONNEG 0   /* 'nonneg': x >= 0, no penalty */
+#define CTPRJ_PROX_TV_ISO 1   /* 'tviso': u TV_iso(x) + (x >= 0), TV.denoise(..., 'iso') */
+#define CTPRJ_PROX_TV_L1 2    /* 'tvl1':  u TV_l1(x) + (x >= 0), TV.denoise(..., 'l1') */
+
 typedef struct {
     int iterations;             /* alternating iterations */
     double x_step;              /* initial density step 1/t (<= 0: 1) */
@@ -51,6 +56,10 @@ typedef struct {
                                    min_iterations have run (bhc/beamhardenSpline.m:
                                    563-566); <= 0: run `iterations` */
     int min_iterations;
+    int proximal;               /* CTPRJ_PROX_* */
+    double u;                   /* penalty weight of the TV proximal maps (opt.u) */
+    int max_inner;              /* first maxInnerItr of the TV map (<= 0: 100, npg/NPG.m:23);
+                                   its tolerance is admmTol * difAlpha, admmTol = 1e-2 */
 } ctprj_bhc_loop_opts;
 
 typedef struct {
@@ -68,6 +77,10 @@ typedef struct {
     int newton_steps;                         /* accepted spectrum Newton steps */
     int converged;                            /* 1: stopped by the thresh rule */
     double x_change[CTPRJ_BHC_LOOP_MAX_TRACE];  /* |x_new - x| / |x| of each iteration */
+    int inner_iterations;                     /* TV denoising iterations, all steps */
+    int prox_retries;                         /* steps retried with a tighter TV map
+                                                 (admmTol / 10 or maxInnerItr * 10) */
+    double penalty;                           /* u TV of the last density candidate */
 } ctprj_bhc_loop_stats;
 
 /* Spectrum update on the projections of the last forward saved by the model

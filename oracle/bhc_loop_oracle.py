@@ -8,7 +8,9 @@ oracle.backward):
 * density step: the reference's NPG class (npg/NPG.m:45-146) or PG class
   (npg/PG.m:41-124) with the projection on x >= 0 as the proximal map, the
   majorisation test of utils/Utils.m:470-480, and the initial step rules of
-  npg/Methods.m:98-124 ('fixed', 'bb', 'hessian');
+  npg/Methods.m:98-124 ('fixed', 'bb', 'hessian'); with proximal 'tviso' /
+  'tvl1' the proximal map is the TV denoising of utils/TV.m (tv_oracle) and the
+  objective carries u TV(x);
 * spectrum step: Newton steps on Ie >= 0 for the objective of bhc/poissLI.m
   (Gauss-Newton curvature for bhc/gaussLI.m), each minimising the quadratic
   model over Ie >= 0 with a primal active-set method on a diagonally lifted,
@@ -24,6 +26,7 @@ import math
 import numpy as np
 
 from . import bhc_oracle as BO
+from . import tv_oracle as TV
 
 
 def _cholesky_lifted(M, lift):
@@ -173,10 +176,18 @@ class _Density:
 
 def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, newton_steps=2,
                 method="npg", init_step="fixed", noise="poisson", skip_spectrum=False, thresh=0.0,
-                min_iterations=0):
+                min_iterations=0, proximal="nonneg", u=0.0, max_inner=100):
     """The alternating loop; forward(x) -> sinogram and backward(sino) -> image
     are FP64 projector callables.  Returns (x, Ie, stats) with stats holding
-    the cost and accepted density step of every iteration."""
+    the cost and accepted density step of every iteration.
+
+    proximal "tviso" / "tvl1" regularises the density with u TV(x): the
+    density step's proximal map becomes TV.denoise (utils/TV.m:56-80, the
+    FGP of tv_oracle.tv_denoise with lambda = u/t, bounds [0, inf),
+    epsilon = admmTol * difAlpha, maxInnerItr iterations), the objective
+    f + u TV, and a rejected step is retried with admmTol / 10 (down to 1e-6)
+    or, when the inner iteration ran out, maxInnerItr * 10 (up to 1000) before
+    x is kept (npg/NPG.m:99-134, npg/PG.m:97-121)."""
     dens = _Density(forward, backward, k, Ts, imea, noise)
     x = np.asarray(x, np.float64).copy()
     Ie = np.asarray(Ie, np.float64).copy()
@@ -198,13 +209,34 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
         if t == 0.0:
             t = np.finfo(np.float64).eps
     pg = method == "pg"
+    tv = proximal != "nonneg"
+    tvkind = "iso" if proximal == "tviso" else "l1"
+    shape = x.shape if x.ndim == 2 else (int(round(math.sqrt(x.size))),) * 2
+    tlv = lambda v: TV.tlv(v.reshape(shape), tvkind) if tv else 0.0
+    admm_tol, dif_alpha, pen = 1e-2, 1.0, 0.0
+    inner = 0
     theta, cost, p, cumu, cumu_tol = 0.0, math.inf, 0, 0, 4
     xprev = x.copy()
     costs, steps, changes = [], [], []
     conv, converged = 0, False
+    inner_total, retries = 0, 0
+
+    def retry():
+        nonlocal admm_tol, max_inner, retries
+        if inner < max_inner and admm_tol > 1e-6:
+            admm_tol /= 10.0
+        elif inner >= max_inner and max_inner < 1000:
+            max_inner *= 10
+        else:
+            return False
+        retries += 1
+        return True
+
+    max_pass = 12 if tv else 3
     for it in range(iterations):
         moved = False
-        for pass_ in range(3):
+        for pass_ in range(max_pass):
+            last = pass_ == max_pass - 1
             p += 1
             theta1 = (1.0 + math.sqrt(1.0 + 4.0 * theta * theta)) / 2.0
             coef = 0.0 if pg else (theta - 1.0) / theta1
@@ -217,7 +249,14 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                 cumu, inc = 0, True
             while True:
                 ppp += 1
-                xn = np.maximum(0.0, xbar - g / t)
+                if tv:
+                    v = (xbar - g / t).reshape(shape)
+                    xn, inner = TV.tv_denoise(v, u / t, 0.0, math.inf, tvkind, max_inner,
+                                              admm_tol * dif_alpha)
+                    xn = xn.reshape(xbar.shape)
+                    inner_total += inner
+                else:
+                    xn = np.maximum(0.0, xbar - g / t)
                 dx = xn - xbar
                 nc = dens.f(xn, Ie)
                 if nc - f0 <= float((g * dx).sum()) + 0.5 * t * float((dx * dx).sum()):
@@ -234,29 +273,42 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                 else:
                     good_mm = False
                     break
+            pen = u * tlv(xn)
+            new_obj = nc + pen
             moved = True
             if pg:
-                if not good_mm or nc > cost:
+                if not good_mm or new_obj > cost:
+                    if tv and not last and retry():
+                        continue
                     moved = False
-            elif nc > cost:
-                if good_mm and mom != 0.0 and pass_ < 2:
+            elif new_obj > cost:
+                if good_mm and mom != 0.0 and not last:
                     theta = 1.0
                     continue
-                if not good_mm or f0 < nc:
+                if not good_mm or f0 + u * tlv(xbar) < new_obj:
+                    if not good_mm:
+                        theta = 1.0
+                    if tv and not last and retry():
+                        continue
                     moved = False
             if not moved:
-                nc = cost
+                new_obj = cost
             theta = theta1
             xprev = x
             if moved:
                 x = xn
+            if tv:
+                dif_alpha = float(np.linalg.norm(xprev - x)) / max(float(np.linalg.norm(x)), 1e-10)
             cumu = cumu + 1 if ppp == 1 else 0
             break
-        cost = nc
+        cost = new_obj
         steps.append(1.0 / t if moved else 0.0)
         if not skip_spectrum:
             A, _, _ = BO.b1_basis(k, dens.s(x), derivs=0)
             Ie, cost, _ = spectrum_steps(A, imea, Ie, newton_steps, noise)
+            # alphaStep.cost = IeStep.cost + u fVal(3) (bhc/beamhardenSpline.m:460): the
+            # penalty of the last candidate, also when it was not accepted
+            cost += pen
         costs.append(cost)
         # relativeDif(x_new, x) and the stopping rule of bhc/beamhardenSpline.m:563-566
         change = float(np.linalg.norm(x - xprev)) / max(float(np.linalg.norm(xprev)), 1e-10)
@@ -267,4 +319,5 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
             converged = True
             break
     return x, Ie, {"cost": costs, "x_step": steps, "final_x_step": 1.0 / t, "x_change": changes,
-                   "converged": converged}
+                   "converged": converged, "inner_iterations": inner_total, "prox_retries": retries,
+                   "penalty": pen}
