@@ -448,7 +448,8 @@ def loop_leg(ct, g, pr, iters):
     (npg/PG.m with the projection on x >= 0, majorisation line search) and an
     FP64 non-negative spectrum step (Newton with an active-set QP on Ie >= 0),
     on the fused path and on the plain FP32 unfused path, then the same with
-    the reference's default accelerated density step (npg/NPG.m); iterations
+    the reference's default accelerated density step (npg/NPG.m), and NPG with
+    the isotropic TV proximal map (opt.proximal = 'tviso', u = 1e-3); iterations
     per second, likelihood evaluations, spectrum time, and how far apart the
     fused and unfused results are."""
     import torch
@@ -469,17 +470,19 @@ def loop_leg(ct, g, pr, iters):
                        "Ie uniform; %d iterations of density step + spectrum step (<= 2 Newton steps)"
                        % (g.n, g.np, g.prjWidth, g.d, iters)}
     res = {}
-    for name, method, unfused in (("pg_fused", "pg", False), ("pg_unfused", "pg", True),
-                                  ("npg_fused", "npg", False)):
+    for name, method, unfused, prox in (("pg_fused", "pg", False, "nonneg"), ("pg_unfused", "pg", True, "nonneg"),
+                                        ("npg_fused", "npg", False, "nonneg"),
+                                        ("npg_tviso_fused", "npg", False, "tviso")):
         x = torch.full((g.n, g.n), 1.0, device="cuda")
         Ie = torch.full((J,), 1.0 / J, dtype=torch.float64, device="cuda")
-        st = model.reconstruct(x, Ie, imea, iterations=iters, x_step=1e-3, unfused=unfused, method=method)
+        st = model.reconstruct(x, Ie, imea, iterations=iters, x_step=1e-3, unfused=unfused, method=method,
+                               proximal=prox, u=1e-3)
         res[name] = (x, Ie)
         out[name] = {"iter_per_s": st["iterations"] / (st["ms"] * 1e-3), "ms": st["ms"],
                      "first_cost": st["cost"][0] if st["cost"] else None, "final_cost": st["final_cost"],
                      "evaluations": st["evaluations"], "ms_per_evaluation": st["ms"] / max(st["evaluations"], 1),
                      "ms_spectrum": st["ms_spectrum"], "newton_steps": st["newton_steps"],
-                     "restarts": st["restarts"],
+                     "restarts": st["restarts"], "tv_inner_iterations": st["inner_iterations"],
                      "rel_err_vs_truth_x": (torch.linalg.norm((x - x_true).double())
                                             / torch.linalg.norm(x_true.double())).item()}
     out["pg_speedup_fused_vs_unfused"] = out["pg_fused"]["iter_per_s"] / out["pg_unfused"]["iter_per_s"]
@@ -554,7 +557,8 @@ def batch_leg(ct, flush, stream, steps):
 def extras_leg(ct, g, pr, flush, stream, steps):
     """FBP on the headline geometry, and the double-precision masked parallel
     operator of mParPrj (prj/parPrj.c) on device buffers: 512^2 image, a disc
-    mask, 360 angles over [0, 180) degrees, 727 detectors."""
+    mask, 360 angles over [0, 180) degrees, 727 detectors; and the TV proximal
+    map of the density step (100 FGP iterations on the headline image size)."""
     import ctypes
 
     import numpy as np
@@ -602,6 +606,21 @@ def extras_leg(ct, g, pr, flush, stream, steps):
         d_b.zero_()
         ct.check(L.ctprj_par_backward(ctypes.byref(conf), theta.ctypes.data, vp(d_mask), mask.size,
                                       vp(d_y), vp(d_b), hs))
+    # the TV proximal map (FGP) on the headline image size, 100 iterations (epsilon = 0)
+    xo = torch.rand(g.n, g.n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(9))
+    xd = torch.empty_like(xo)
+    itn = ctypes.c_int(0)
+    tv_iters = 100
+
+    def tv_run():
+        ct.check(L.ctprj_tv_denoise(vp(xo), g.n, g.n, 0.05, 0.0, float("inf"), 0, tv_iters, 0.0, vp(xd),
+                                    ctypes.byref(itn), hs))
+    tv_ms = timed(tv_run)
+    # algorithmic bytes per iteration: the fused iteration reads Xobs, D_old,
+    # P1, P2, P1_prev, P2_prev and writes D, P1_new, P2_new (36 B/pixel)
+    out["tv_denoise"] = {"workload": "isotropic TV FGP on %d^2, lambda 0.05, %d iterations" % (g.n, tv_iters),
+                         "ms": tv_ms, "us_per_iteration": 1e3 * tv_ms / tv_iters,
+                         "algorithmic_GBps": 36.0 * g.n * g.n * tv_iters / (tv_ms * 1e-3) / 1e9}
     out["parprj"] = {"workload": "FP64 masked parallel operator (mParPrj): %d^2 image, disc mask of %d "
                                  "pixels, %d angles over [0,180) deg, %d detectors" % (n, mask.size, nang, W),
                      "forward_ms": timed(fwd), "backward_ms": timed(bwd)}

@@ -35,7 +35,8 @@ class LoopOpts(ctypes.Structure):
                 ("unfused", ctypes.c_int), ("init_step", ctypes.c_int),
                 ("density_method", ctypes.c_int), ("thresh", ctypes.c_double),
                 ("min_iterations", ctypes.c_int), ("proximal", ctypes.c_int),
-                ("u", ctypes.c_double), ("max_inner", ctypes.c_int)]
+                ("u", ctypes.c_double), ("max_inner", ctypes.c_int), ("admm_tol", ctypes.c_double),
+                ("no_restart", ctypes.c_int), ("no_adaptive_step", ctypes.c_int), ("cumu_tol", ctypes.c_int)]
 
 
 class LoopStats(ctypes.Structure):

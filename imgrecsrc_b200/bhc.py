@@ -149,7 +149,7 @@ class BHCModel:
     def reconstruct(self, x, Ie, imea, iterations, x_step=1.0, spectrum_newton_steps=2,
                     skip_spectrum=False, unfused=False, init_step="fixed", method="npg",
                     thresh=0.0, min_iterations=0, proximal="nonneg", u=0.0, max_inner=100,
-                    stream=None):
+                    admm_tol=1e-2, restart=True, adaptive_step=True, cumu_tol=4, stream=None):
         """The alternating density / spectrum loop, x and Ie updated in place.
         init_step: 'fixed' (first step x_step), 'bb' or 'hessian' (the
         reference's stepSizeInit rules); method: 'npg' (npg/NPG.m) or 'pg'
@@ -157,8 +157,10 @@ class BHCModel:
         reference's rule (relative density change <= thresh in three
         iterations after the first, more than min_iterations run);
         proximal: 'nonneg', 'tviso' or 'tvl1' (the reference's opt.proximal
-        for NPG / PG), the TV maps with penalty weight u and a first inner
-        iteration limit max_inner.
+        for NPG / PG), the TV maps with penalty weight u, a first inner
+        iteration limit max_inner and a first inner tolerance scale admm_tol;
+        restart, adaptive_step and cumu_tol are the reference's opt.restart,
+        opt.adaptiveStep and opt.cumuTol.
         Returns a dict with the cost after each iteration, the accepted density
         steps and the device time."""
         import torch
@@ -167,7 +169,8 @@ class BHCModel:
                         1 if skip_spectrum else 0, 1 if unfused else 0,
                         {"fixed": 0, "bb": 1, "hessian": 2}[init_step], {"npg": 0, "pg": 1}[method],
                         float(thresh), int(min_iterations),
-                        {"nonneg": 0, "tviso": 1, "tvl1": 2}[proximal], float(u), int(max_inner))
+                        {"nonneg": 0, "tviso": 1, "tvl1": 2}[proximal], float(u), int(max_inner),
+                        float(admm_tol), 0 if restart else 1, 0 if adaptive_step else 1, int(cumu_tol))
         st = LoopStats()
         check(lib().ctprj_bhc_reconstruct(self._m, _dev_ptr(x, pr.img_shape, pr.device),
                                           _dptr(Ie, self.J, torch.float64),

@@ -807,6 +807,8 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         return set_error(CTPRJ_EINVAL, "unknown proximal map %d", prox);
     const bool tv = prox != CTPRJ_PROX_NONNEG;
     if (tv && !(opts->u > 0.0)) return set_error(CTPRJ_EINVAL, "the TV proximal maps need u > 0");
+    if (tv && (long long)m->plan->g.n * m->plan->g.n >= (1LL << 31))
+        return set_error(CTPRJ_EINVAL, "the TV proximal maps need an image below 2^31 pixels");
     PlanDevice pd(m->plan->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long npx = (long long)m->plan->g.n * m->plan->g.n;
@@ -839,13 +841,15 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     const bool pg = opts->density_method == CTPRJ_DENSITY_PG;
     double t = 1.0 / (opts->x_step > 0 ? opts->x_step : 1.0);   // inverse step size
     double theta = 0.0, cost = INFINITY;
-    int p = 0, cumu = 0, cumu_tol = 4, evals = 0, restarts = 0, newton_done = 0, conv = 0, converged = 0;
+    int p = 0, cumu = 0, cumu_tol = opts->cumu_tol > 0 ? opts->cumu_tol : 4, evals = 0, restarts = 0,
+        newton_done = 0, conv = 0, converged = 0;
+    const bool adaptive = !opts->no_adaptive_step, restart_on = !opts->no_restart;
     const int pre_steps = 10;
     const double shrink = 0.5;
     // the TV proximal map's state (npg/NPG.m:11,23-24 and Methods.m difAlpha = 1)
     const bool iso = prox == CTPRJ_PROX_TV_ISO;
     const int max_pass = tv ? 12 : 3;
-    double admm_tol = 1e-2, dif_alpha = 1.0, pen = 0.0;
+    double admm_tol = opts->admm_tol > 0.0 ? opts->admm_tol : 1e-2, dif_alpha = 1.0, pen = 0.0;
     int max_inner = opts->max_inner > 0 ? opts->max_inner : 100, inner = 0, inner_total = 0, retries = 0;
     auto penalty_of = [&](const float *v, double *out) -> int {   // u TV(v)
         double tvv = 0.0;
@@ -872,7 +876,11 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     cudaEventCreate(&e1);
     cudaEventCreate(&es0);
     cudaEventCreate(&es1);
-    st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "loop start");
+    // alpha = max(alpha, 0) before the NPG / PG object is built (bhc/beamhardenSpline.m:232,236)
+    k_npg_extrapolate<<<pgb, 256, 0, s>>>(d_x, d_x, npx, 0.0f, d_x, b.part);
+    st = cuda_error(cudaGetLastError(), "loop start");
+    if (!st)
+        st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "loop start");
     cudaEventRecord(e0, s);
     if (!st && opts->init_step != CTPRJ_STEP_FIXED) {
         st = initial_inverse_step(m, d_x, d_Ie, d_imea, opts->init_step, b, pgb, &t, s);
@@ -899,7 +907,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             ++evals;
             int ppp = 0;
             bool good = true, inc = false, good_mm = true;
-            if (cumu >= cumu_tol) {   // adaptively grow the step
+            if (adaptive && cumu >= cumu_tol) {   // adaptively grow the step
                 t *= shrink;
                 cumu = 0;
                 inc = true;
@@ -954,7 +962,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                     moved = false;                          // npg/PG.m: force convergence
                 }
             } else if (obj > cost) {
-                if (good_mm && mom != 0.0 && !last) {      // restart without momentum
+                if (good_mm && mom != 0.0 && restart_on && !last) {   // restart without momentum
                     theta = 1.0;
                     ++restarts;
                     continue;
@@ -980,7 +988,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                     dif_alpha = sqrt(dq[0]) / fmax(sqrt(dq[1]), 1e-10);
             }
             state_at_x = moved;   // the last likelihood evaluated (and saved) was at xn
-            cumu = ppp == 1 ? cumu + 1 : 0;
+            cumu = (ppp == 1 && adaptive) ? cumu + 1 : 0;
             break;
         }
         if (st) break;

@@ -58,8 +58,13 @@ typedef struct {
     int min_iterations;
     int proximal;               /* CTPRJ_PROX_* */
     double u;                   /* penalty weight of the TV proximal maps (opt.u) */
-    int max_inner;              /* first maxInnerItr of the TV map (<= 0: 100, npg/NPG.m:23);
-                                   its tolerance is admmTol * difAlpha, admmTol = 1e-2 */
+    int max_inner;              /* first maxInnerItr of the TV map (<= 0: 100, npg/NPG.m:23) */
+    double admm_tol;            /* first admmTol (opt.admmTol; <= 0: 1e-2, npg/NPG.m:11);
+                                   the TV map's tolerance is admmTol * difAlpha */
+    int no_restart;             /* 1: opt.restart = false (NPG without momentum restart) */
+    int no_adaptive_step;       /* 1: opt.adaptiveStep = false (no step growth after
+                                   cumu_tol first-try successes) */
+    int cumu_tol;               /* opt.cumuTol (<= 0: 4) */
 } ctprj_bhc_loop_opts;
 
 typedef struct {

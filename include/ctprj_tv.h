@@ -40,7 +40,7 @@ extern "C" {
  * (utils/denoise_bound_mod.m:1; TV.denoise, utils/TV.m:56, passes
  * lb = 0, ub = inf).  ub may be +INFINITY.  d_out (rows*cols floats) may not
  * alias d_xobs.  *iterations (may be NULL) receives iter.  Needs rows, cols
- * >= 2, lambda > 0, lb < ub. */
+ * >= 2, rows * cols < 2^31, lambda > 0, lb < ub. */
 int ctprj_tv_denoise(const float *d_xobs, int rows, int cols, double lambda, double lb, double ub,
                      int tv_type, int max_iter, double epsilon, float *d_out, int *iterations,
                      void *stream);

@@ -176,7 +176,8 @@ class _Density:
 
 def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, newton_steps=2,
                 method="npg", init_step="fixed", noise="poisson", skip_spectrum=False, thresh=0.0,
-                min_iterations=0, proximal="nonneg", u=0.0, max_inner=100):
+                min_iterations=0, proximal="nonneg", u=0.0, max_inner=100, admm_tol=1e-2, restart=True,
+                adaptive_step=True, cumu_tol=4):
     """The alternating loop; forward(x) -> sinogram and backward(sino) -> image
     are FP64 projector callables.  Returns (x, Ie, stats) with stats holding
     the cost and accepted density step of every iteration.
@@ -187,9 +188,11 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
     epsilon = admmTol * difAlpha, maxInnerItr iterations), the objective
     f + u TV, and a rejected step is retried with admmTol / 10 (down to 1e-6)
     or, when the inner iteration ran out, maxInnerItr * 10 (up to 1000) before
-    x is kept (npg/NPG.m:99-134, npg/PG.m:97-121)."""
+    x is kept (npg/NPG.m:99-134, npg/PG.m:97-121).  restart, adaptive_step,
+    cumu_tol and admm_tol are the reference's opt.restart, opt.adaptiveStep,
+    opt.cumuTol and opt.admmTol (bhc/beamhardenSpline.m:277-294)."""
     dens = _Density(forward, backward, k, Ts, imea, noise)
-    x = np.asarray(x, np.float64).copy()
+    x = np.maximum(np.asarray(x, np.float64), 0.0)     # alpha = max(alpha, 0): :232, :236
     Ie = np.asarray(Ie, np.float64).copy()
     t = 1.0 / (x_step if x_step > 0 else 1.0)
     if init_step != "fixed":
@@ -213,9 +216,9 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
     tvkind = "iso" if proximal == "tviso" else "l1"
     shape = x.shape if x.ndim == 2 else (int(round(math.sqrt(x.size))),) * 2
     tlv = lambda v: TV.tlv(v.reshape(shape), tvkind) if tv else 0.0
-    admm_tol, dif_alpha, pen = 1e-2, 1.0, 0.0
+    dif_alpha, pen = 1.0, 0.0
     inner = 0
-    theta, cost, p, cumu, cumu_tol = 0.0, math.inf, 0, 0, 4
+    theta, cost, p, cumu = 0.0, math.inf, 0, 0
     xprev = x.copy()
     costs, steps, changes = [], [], []
     conv, converged = 0, False
@@ -244,7 +247,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
             mom = float(np.abs(xbar - x).sum())
             f0, g = dens.f(xbar, Ie, grad=True)
             ppp, good, inc, good_mm = 0, True, False, True
-            if cumu >= cumu_tol:
+            if adaptive_step and cumu >= cumu_tol:
                 t *= 0.5
                 cumu, inc = 0, True
             while True:
@@ -282,7 +285,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                         continue
                     moved = False
             elif new_obj > cost:
-                if good_mm and mom != 0.0 and not last:
+                if good_mm and mom != 0.0 and restart and not last:
                     theta = 1.0
                     continue
                 if not good_mm or f0 + u * tlv(xbar) < new_obj:
@@ -299,7 +302,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                 x = xn
             if tv:
                 dif_alpha = float(np.linalg.norm(xprev - x)) / max(float(np.linalg.norm(x)), 1e-10)
-            cumu = cumu + 1 if ppp == 1 else 0
+            cumu = cumu + 1 if ppp == 1 and adaptive_step else 0
             break
         cost = new_obj
         steps.append(1.0 / t if moved else 0.0)
