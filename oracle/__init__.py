@@ -58,6 +58,15 @@ def build_ref(ref_prj_dir="/root/reference/prj"):
     return True
 
 
+def build_rwt(ref_rwt_dir="/root/reference/rwt"):
+    """The reference's vendored wavelet transform cores (rwt/mdwt_r.c,
+    rwt/midwt_r.c), compiled unchanged into oracle/_ref/libref_rwt.so."""
+    if not os.path.isdir(ref_rwt_dir):
+        return False
+    subprocess.run(["make", "-s", "-C", HERE, "rwt", "RWT=" + ref_rwt_dir], check=True)
+    return True
+
+
 def build_gateways(ref_prj_dir="/root/reference/prj"):
     """The reference's own MEX gateways compiled against the engine library
     (oracle/Makefile target `gateways`), for the boundary tests."""
