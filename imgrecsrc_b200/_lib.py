@@ -139,6 +139,11 @@ def lib():
                               ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, VP,
                               ctypes.POINTER(ctypes.c_int), VP], ctypes.c_int),
         "ctprj_tv_value": ([VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, VP, VP], ctypes.c_int),
+        "ctprj_dwt": ([VP, ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, VP, VP], ctypes.c_int),
+        "ctprj_idwt": ([VP, ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, VP, VP], ctypes.c_int),
+        "ctprj_wvlt_l1": ([VP, ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, VP, VP], ctypes.c_int),
+        "ctprj_wvlt_admm": ([VP, ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                             ctypes.c_double, ctypes.c_int, VP, VP, ctypes.POINTER(ctypes.c_int), VP], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

@@ -218,6 +218,23 @@ int tv_denoise(TvWorkspace &ws, const float *xobs, int m, int n, double lambda, 
 // *d_out = TV(x) in FP64 (device)
 int tv_value(TvWorkspace &ws, const float *x, int m, int n, int iso, double *d_out, cudaStream_t s);
 
+// buffers of the wavelet ADMM proximal map (wavelet.cu): LL scratch (half an
+// image), s (two), nu; per-block FP64 partials; the device-side ADMM state
+struct WvltProx {
+    float *buf = nullptr;
+    double *part = nullptr;
+    void *state = nullptr;
+    int rows = 0, cols = 0;
+    int alloc(int m, int n, cudaStream_t s);
+    void release(cudaStream_t s);
+};
+// alpha = argmin 1/2 |alpha - a|^2 + I(alpha >= 0) + u |W alpha|_1 by npg/admm.m
+int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h, int lh, int levels, double u,
+              double rel_tol, int max_itr, const float *init, float *alpha, int *iterations, cudaStream_t s);
+// *d_out = |W x|_1 in FP64 (device)
+int wvlt_l1(WvltProx &ws, const float *x, int rows, int cols, const double *h, int lh, int levels, double *d_out,
+            cudaStream_t s);
+
 // launchers (projector.cu)
 // the quad image of the forward pass (projector.cu): (half + 1) rows of
 // 2 half + 1 float4, built in 32 x 32 tiles

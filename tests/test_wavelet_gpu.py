@@ -1,0 +1,145 @@
+"""The wavelet transform and the ADMM wavelet proximal map on the GPU
+(include/ctprj_wavelet.h) against the reference's compiled rwt cores
+(tests/golden/rwt_golden.npz) and the FP64 restatement of npg/admm.m
+(oracle/wavelet_oracle.py)."""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from oracle import wavelet_oracle as W
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import imgrecsrc_b200 as ct  # noqa: E402
+from imgrecsrc_b200 import wavelet  # noqa: E402
+from imgrecsrc_b200._lib import CtprjError  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rwt_golden.npz")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def rel(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x, np.float32)).cuda()
+
+
+def test_transforms_match_the_compiled_reference():
+    """Every golden case (Haar to 12 taps, 2 to 6 levels, filters longer than
+    the coarsest block): FP32 transforms within 1e-6 of the reference's
+    double-precision MDWT / MIDWT."""
+    g = np.load(GOLDEN)
+    i = 0
+    while "case%d_meta" % i in g:
+        daub, m, n, L = (int(v) for v in g["case%d_meta" % i])
+        h = g["case%d_h" % i]
+        x = dev(g["case%d_x" % i])
+        y = wavelet.mdwt(x, h, L).cpu().numpy()
+        xi = wavelet.midwt(x, h, L).cpu().numpy()
+        e1, e2 = rel(y, g["case%d_mdwt" % i]), rel(xi, g["case%d_midwt" % i])
+        print("rwt case %d (daub %d, %dx%d, L %d): mdwt %.2e midwt %.2e" % (i, daub, m, n, L, e1, e2))
+        assert e1 < 1e-6 and e2 < 1e-6
+        i += 1
+    assert i >= 7
+
+
+@pytest.mark.parametrize("daub,shape,L", [(2, (1024, 1024), 6), (4, (512, 768), 5), (8, (256, 128), 4)])
+def test_large_transforms_and_inverse(daub, shape, L):
+    rng = np.random.default_rng(daub)
+    X = rng.standard_normal(shape)
+    h = W.daubcqf(daub)
+    y = wavelet.mdwt(dev(X), h, L)
+    e = rel(y.cpu().numpy(), W.mdwt(X, h, L))
+    xi = wavelet.midwt(y, h, L).cpu().numpy()
+    print("daub %d %s L %d: mdwt rel %.2e, round trip %.2e" % (daub, shape, L, e, rel(xi, X)))
+    assert e < 1e-6
+    assert rel(xi, X) < 2e-6
+
+
+def test_transposed_layout_gives_the_matlab_coefficients():
+    """A column-major (MATLAB) array passed as it lies, rows and columns
+    swapped: the result read column-major is MATLAB's mdwt."""
+    rng = np.random.default_rng(5)
+    X = rng.standard_normal((64, 32))                 # MATLAB 64 x 32
+    h = W.daubcqf(4)
+    mem = dev(X.T)                                    # its memory, row-major 32 x 64
+    y = wavelet.mdwt(mem, h, 3).cpu().numpy().T
+    assert rel(y, W.mdwt(X, h, 3)) < 1e-6
+
+
+@pytest.mark.parametrize("daub", [2, 6])
+def test_l1_penalty(daub):
+    rng = np.random.default_rng(6)
+    X = rng.standard_normal((128, 64))
+    h = W.daubcqf(daub)
+    v = wavelet.l1(dev(X), h, 4)
+    vo = W.l1_penalty(X.astype(np.float32).astype(np.float64), h, 4)
+    assert abs(v - vo) / vo < 1e-6
+
+
+def phantomish(n, seed):
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:n, 0:n]
+    img = ((xx - n / 2) ** 2 + (yy - n / 2) ** 2 < (n / 3) ** 2).astype(np.float64)
+    img += 0.7 * ((xx > n / 5) & (xx < n / 2) & (yy > n / 4) & (yy < n / 2))
+    return img + 0.1 * rng.standard_normal((n, n))
+
+
+@pytest.mark.parametrize("daub,u", [(2, 0.5), (4, 0.2)])
+def test_admm_fixed_iterations_match_the_fp64_restatement(daub, u):
+    """relativeTol = 0: both run maxItr + 1 iterations of the same ADMM
+    (including rho adaptations after 20 iterations); alpha agrees to FP32
+    accuracy."""
+    a = phantomish(64, daub) - 0.2
+    init = np.maximum(phantomish(64, daub + 1), 0.0)
+    h = W.daubcqf(daub)
+    al, it = wavelet.admm(dev(a), u, h, 5, relative_tol=0.0, max_itr=60, init=dev(init))
+    alo, ito = W.admm(a.astype(np.float32).astype(np.float64), u, h, 5, rel_tol=0.0, max_itr=60,
+                      init=init.astype(np.float32).astype(np.float64))
+    e = rel(al.cpu().numpy(), alo)
+    print("ADMM daub %d u %g: %d / %d iterations, alpha rel %.2e" % (daub, u, it, ito, e))
+    assert it == ito == 61
+    assert e < 1e-4
+    assert al.min().item() >= 0.0
+
+
+def test_admm_stopping_rule_and_objective():
+    """With the tolerances the density step passes (1e-3 down), the FP32
+    iteration stops within a few iterations of the FP64 one and reaches the
+    same objective 1/2 |alpha - a|^2 + u |W alpha|_1 to 1e-5."""
+    a = phantomish(128, 9) - 0.1
+    h = W.daubcqf(2)
+    for tol in (1e-3, 1e-5):
+        al, it = wavelet.admm(dev(a), 0.3, h, 6, relative_tol=tol, max_itr=1000)
+        a64 = a.astype(np.float32).astype(np.float64)
+        alo, ito = W.admm(a64, 0.3, h, 6, rel_tol=tol, max_itr=1000)
+        f = W.admm_objective(al.cpu().numpy().astype(np.float64), a64, 0.3, h, 6)
+        fo = W.admm_objective(alo, a64, 0.3, h, 6)
+        print("ADMM tol %g: gpu %d iterations, oracle %d; objective rel %.2e" % (tol, it, ito, abs(f - fo) / fo))
+        assert abs(it - ito) <= max(3, 0.1 * ito)
+        assert abs(f - fo) / fo < 1e-5
+
+
+def test_admm_zero_input_and_errors():
+    z = torch.zeros(32, 32, device="cuda")
+    out, it = wavelet.admm(z, 0.1, W.daubcqf(2), 3)
+    assert it == 0 and not out.any().item()
+    x = torch.zeros(24, 24, device="cuda")
+    with pytest.raises(CtprjError):
+        wavelet.mdwt(x, W.daubcqf(2), 4)               # 24 not divisible by 16
+    with pytest.raises(CtprjError):
+        wavelet.mdwt(x, np.ones(3), 1)                # odd filter
+    with pytest.raises(CtprjError):
+        wavelet.admm(x, -1.0, W.daubcqf(2), 2)        # negative weight
