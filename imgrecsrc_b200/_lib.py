@@ -36,7 +36,9 @@ class LoopOpts(ctypes.Structure):
                 ("density_method", ctypes.c_int), ("thresh", ctypes.c_double),
                 ("min_iterations", ctypes.c_int), ("proximal", ctypes.c_int),
                 ("u", ctypes.c_double), ("max_inner", ctypes.c_int), ("admm_tol", ctypes.c_double),
-                ("no_restart", ctypes.c_int), ("no_adaptive_step", ctypes.c_int), ("cumu_tol", ctypes.c_int)]
+                ("no_restart", ctypes.c_int), ("no_adaptive_step", ctypes.c_int), ("cumu_tol", ctypes.c_int),
+                ("wvlt_filter_len", ctypes.c_int), ("wvlt_filter", ctypes.c_double * 20),
+                ("wvlt_levels", ctypes.c_int)]
 
 
 class LoopStats(ctypes.Structure):

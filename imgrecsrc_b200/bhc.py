@@ -149,7 +149,8 @@ class BHCModel:
     def reconstruct(self, x, Ie, imea, iterations, x_step=1.0, spectrum_newton_steps=2,
                     skip_spectrum=False, unfused=False, init_step="fixed", method="npg",
                     thresh=0.0, min_iterations=0, proximal="nonneg", u=0.0, max_inner=100,
-                    admm_tol=1e-2, restart=True, adaptive_step=True, cumu_tol=4, stream=None):
+                    admm_tol=1e-2, restart=True, adaptive_step=True, cumu_tol=4, wvlt_filter=None,
+                    wvlt_levels=6, stream=None):
         """The alternating density / spectrum loop, x and Ie updated in place.
         init_step: 'fixed' (first step x_step), 'bb' or 'hessian' (the
         reference's stepSizeInit rules); method: 'npg' (npg/NPG.m) or 'pg'
@@ -160,7 +161,9 @@ class BHCModel:
         for NPG / PG), the TV maps with penalty weight u, a first inner
         iteration limit max_inner and a first inner tolerance scale admm_tol;
         restart, adaptive_step and cumu_tol are the reference's opt.restart,
-        opt.adaptiveStep and opt.cumuTol.
+        opt.adaptiveStep and opt.cumuTol.  proximal 'wvltADMM' (the reference's
+        default) regularises with u |Psit(x)|_1 for the wavelet of scaling
+        filter wvlt_filter (default daubcqf(2), Haar) and wvlt_levels levels.
         Returns a dict with the cost after each iteration, the accepted density
         steps and the device time."""
         import torch
@@ -169,8 +172,17 @@ class BHCModel:
                         1 if skip_spectrum else 0, 1 if unfused else 0,
                         {"fixed": 0, "bb": 1, "hessian": 2}[init_step], {"npg": 0, "pg": 1}[method],
                         float(thresh), int(min_iterations),
-                        {"nonneg": 0, "tviso": 1, "tvl1": 2}[proximal], float(u), int(max_inner),
-                        float(admm_tol), 0 if restart else 1, 0 if adaptive_step else 1, int(cumu_tol))
+                        {"nonneg": 0, "tviso": 1, "tvl1": 2, "wvltadmm": 3}[proximal.lower()], float(u),
+                        int(max_inner), float(admm_tol), 0 if restart else 1, 0 if adaptive_step else 1,
+                        int(cumu_tol))
+        if wvlt_filter is not None:
+            wf = np.asarray(wvlt_filter, np.float64)
+            if wf.size > 20:
+                raise ValueError("wavelet filters of at most 20 taps")
+            opts.wvlt_filter_len = wf.size
+            for j, v in enumerate(wf):
+                opts.wvlt_filter[j] = float(v)
+        opts.wvlt_levels = int(wvlt_levels)
         st = LoopStats()
         check(lib().ctprj_bhc_reconstruct(self._m, _dev_ptr(x, pr.img_shape, pr.device),
                                           _dptr(Ie, self.J, torch.float64),

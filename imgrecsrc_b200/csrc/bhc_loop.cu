@@ -803,12 +803,27 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     if (!m || !d_x || !d_Ie || !d_imea || !opts) return set_error(CTPRJ_EINVAL, "NULL argument");
     if (opts->iterations < 0) return set_error(CTPRJ_EINVAL, "negative iteration count");
     const int prox = opts->proximal;
-    if (prox != CTPRJ_PROX_NONNEG && prox != CTPRJ_PROX_TV_ISO && prox != CTPRJ_PROX_TV_L1)
+    if (prox != CTPRJ_PROX_NONNEG && prox != CTPRJ_PROX_TV_ISO && prox != CTPRJ_PROX_TV_L1 &&
+        prox != CTPRJ_PROX_WVLT_ADMM)
         return set_error(CTPRJ_EINVAL, "unknown proximal map %d", prox);
-    const bool tv = prox != CTPRJ_PROX_NONNEG;
-    if (tv && !(opts->u > 0.0)) return set_error(CTPRJ_EINVAL, "the TV proximal maps need u > 0");
-    if (tv && (long long)m->plan->g.n * m->plan->g.n >= (1LL << 31))
-        return set_error(CTPRJ_EINVAL, "the TV proximal maps need an image below 2^31 pixels");
+    const bool tv = prox == CTPRJ_PROX_TV_ISO || prox == CTPRJ_PROX_TV_L1;
+    const bool wv = prox == CTPRJ_PROX_WVLT_ADMM;
+    const bool reg = tv || wv;   // a regulariser with an iterative proximal map
+    if (reg && !(opts->u > 0.0)) return set_error(CTPRJ_EINVAL, "the regularised proximal maps need u > 0");
+    if (reg && (long long)m->plan->g.n * m->plan->g.n >= (1LL << 31))
+        return set_error(CTPRJ_EINVAL, "the regularised proximal maps need an image below 2^31 pixels");
+    // the wavelet: Utils.getPsiPsit(daub, dwt_L) filter and levels, by default
+    // daub = 2 (Haar) and dwt_L = 6 as the reference's BHC runs (bhc/doBHC.m:33)
+    double wh[CTPRJ_WVLT_MAX_FILTER];
+    const int wlh = opts->wvlt_filter_len > 0 ? opts->wvlt_filter_len : 2;
+    const int wlev = opts->wvlt_levels > 0 ? opts->wvlt_levels : 6;
+    if (wv) {
+        if (wlh > CTPRJ_WVLT_MAX_FILTER || (wlh & 1))
+            return set_error(CTPRJ_EINVAL, "wavelet filter length %d: even, at most %d", wlh, CTPRJ_WVLT_MAX_FILTER);
+        for (int j = 0; j < wlh; ++j) wh[j] = opts->wvlt_filter_len > 0 ? opts->wvlt_filter[j] : M_SQRT1_2;
+        if (wlev > 30 || m->plan->g.n % (1 << wlev))
+            return set_error(CTPRJ_EINVAL, "image side %d not divisible by 2^%d wavelet levels", m->plan->g.n, wlev);
+    }
     PlanDevice pd(m->plan->device);
     cudaStream_t s = (cudaStream_t)stream;
     const long long npx = (long long)m->plan->g.n * m->plan->g.n;
@@ -818,6 +833,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     LoopBufs b;
     SpectrumWs ws;
     TvWorkspace tvw;
+    WvltProx wws;
     const int n = m->plan->g.n;
     int st;
     if ((st = cuda_error(cudaMalloc((void **)&b.gx, sizeof(float) * npx), "loop buffers")) ||
@@ -827,12 +843,14 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         (st = cuda_error(cudaMalloc((void **)&b.f, sizeof(double) * 2), "loop buffers")) ||
         (st = cuda_error(cudaMalloc((void **)&b.part, sizeof(double) * 2 * pgb), "loop buffers")) ||
         (st = cuda_error(cudaMalloc((void **)&b.sum, sizeof(double) * 4), "loop buffers")) ||
-        (tv && (st = cuda_error(cudaMalloc((void **)&b.v, sizeof(float) * npx), "loop buffers"))) ||
+        (reg && (st = cuda_error(cudaMalloc((void **)&b.v, sizeof(float) * npx), "loop buffers"))) ||
         (tv && (st = tvw.alloc(n, n, s))) ||
+        (wv && (st = wws.alloc(n, n, s))) ||
         (opts->unfused &&
          (st = cuda_error(cudaMalloc((void **)&b.sino, sizeof(float) * nr), "loop buffers"))) ||
         (!opts->skip_spectrum && (st = ws.alloc(m->J, nr, spectrum_grid(dev), s)))) {
         tvw.release(s);
+        wws.release(s);
         cudaStreamSynchronize(s);
         b.release();
         return st;
@@ -846,19 +864,19 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     const bool adaptive = !opts->no_adaptive_step, restart_on = !opts->no_restart;
     const int pre_steps = 10;
     const double shrink = 0.5;
-    // the TV proximal map's state (npg/NPG.m:11,23-24 and Methods.m difAlpha = 1)
+    // the iterative proximal maps' state (npg/NPG.m:11,23-24 and Methods.m difAlpha = 1)
     const bool iso = prox == CTPRJ_PROX_TV_ISO;
-    const int max_pass = tv ? 12 : 3;
+    const int max_pass = reg ? 12 : 3;
     double admm_tol = opts->admm_tol > 0.0 ? opts->admm_tol : 1e-2, dif_alpha = 1.0, pen = 0.0;
     int max_inner = opts->max_inner > 0 ? opts->max_inner : 100, inner = 0, inner_total = 0, retries = 0;
-    auto penalty_of = [&](const float *v, double *out) -> int {   // u TV(v)
+    auto penalty_of = [&](const float *v, double *out) -> int {   // u TV(v) or u |Psit(v)|_1
         double tvv = 0.0;
-        int e = tv_value(tvw, v, n, n, iso, b.sum + 3, s);
+        int e = tv ? tv_value(tvw, v, n, n, iso, b.sum + 3, s) : wvlt_l1(wws, v, n, n, wh, wlh, wlev, b.sum + 3, s);
         if (!e) e = fetch(&tvv, b.sum + 3, 1, s);
         *out = opts->u * tvv;
         return e;
     };
-    // a rejected TV step is retried with a tighter inner tolerance or, when the
+    // a rejected regularised step is retried with a tighter inner tolerance or, when the
     // inner iteration ran out, more inner iterations (npg/NPG.m:117-128)
     auto retry = [&]() -> bool {
         if (inner < max_inner && admm_tol > 1e-6)
@@ -914,12 +932,16 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             }
             while (true) {
                 ++ppp;
-                if (tv) {   // xn = TV.denoise(xbar - g / t, u / t, admmTol difAlpha, maxInnerItr)
+                if (reg) {   // xn = proxmapping(xbar - g / t, u / t, admmTol difAlpha, maxInnerItr, x)
                     k_axpy<<<pgb, 256, 0, s>>>(b.xbar, b.gx, (float)(-1.0 / t), npx, b.v);
-                    if ((st = cuda_error(cudaGetLastError(), "density step")) ||
-                        (st = tv_denoise(tvw, b.v, n, n, opts->u / t, 0.0, INFINITY, iso, max_inner,
-                                         admm_tol * dif_alpha, b.xn, &inner, s)))
-                        break;
+                    if ((st = cuda_error(cudaGetLastError(), "density step"))) break;
+                    if (tv)   // TV.denoise (utils/TV.m:56-80), which starts from D = 0
+                        st = tv_denoise(tvw, b.v, n, n, opts->u / t, 0.0, INFINITY, iso, max_inner,
+                                        admm_tol * dif_alpha, b.xn, &inner, s);
+                    else      // admm(Psi, Psit, ., init = x) (npg/admm.m)
+                        st = wvlt_admm(wws, b.v, n, n, wh, wlh, wlev, opts->u / t, admm_tol * dif_alpha, max_inner,
+                                       d_x, b.xn, &inner, s);
+                    if (st) break;
                     inner_total += inner;
                     k_step_terms<<<pgb, 256, 0, s>>>(b.xbar, b.gx, b.xn, npx, b.part);
                 } else {
@@ -953,12 +975,12 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                 }
             }
             if (st) break;
-            if (tv && (st = penalty_of(b.xn, &pen))) break;
+            if (reg && (st = penalty_of(b.xn, &pen))) break;
             obj = nc + pen;
             moved = true;
             if (pg) {
                 if (!good_mm || obj > cost) {
-                    if (tv && !last && retry()) continue;
+                    if (reg && !last && retry()) continue;
                     moved = false;                          // npg/PG.m: force convergence
                 }
             } else if (obj > cost) {
@@ -968,10 +990,10 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                     continue;
                 }
                 double pen_bar = 0.0;
-                if (tv && good_mm && (st = penalty_of(b.xbar, &pen_bar))) break;
+                if (reg && good_mm && (st = penalty_of(b.xbar, &pen_bar))) break;
                 if (!good_mm || f0 + pen_bar < obj) {
                     if (!good_mm) theta = 1.0;              // NPG's reset() (its t reset is not taken)
-                    if (tv && !last && retry()) continue;
+                    if (reg && !last && retry()) continue;
                     moved = false;                          // npg/NPG.m: force convergence
                 }
             }
@@ -980,7 +1002,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "accept");
             if (!st && moved)
                 st = cuda_error(cudaMemcpyAsync(d_x, b.xn, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "accept");
-            if (!st && tv) {   // difAlpha = relativeDif(x, x_new), the next inner tolerance's scale
+            if (!st && reg) {   // difAlpha = relativeDif(x, x_new), the next inner tolerance's scale
                 k_rel_change<<<pgb, 256, 0, s>>>(b.xprev, d_x, npx, b.part);
                 k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 2, b.sum);
                 double dq[2];
@@ -1053,6 +1075,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     }
     ws.release(s);
     tvw.release(s);
+    wws.release(s);
     cudaStreamSynchronize(s);
     b.release();
     return st;

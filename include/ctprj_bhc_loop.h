@@ -3,8 +3,9 @@
  *
  * Counterpart of the reference's BHC driver loop (bhc/beamhardenSpline.m:
  * 340-570): one density step on the likelihood (the reference's NPG class,
- * npg/NPG.m, or its PG class, npg/PG.m, with the non-negativity projection or
- * the TV denoising of include/ctprj_tv.h as the proximal map),
+ * npg/NPG.m, or its PG class, npg/PG.m, with the non-negativity projection,
+ * the TV denoising of include/ctprj_tv.h or the wavelet ADMM of
+ * include/ctprj_wavelet.h as the proximal map),
  * then a non-negative spectrum step, repeated.  Built on the model of
  * include/ctprj.h (ctprj_bhc_*): every likelihood and gradient of the density
  * step comes from the fused forward projection and its adjoint; the spectrum
@@ -17,6 +18,7 @@
 #define CTPRJ_BHC_LOOP_H
 
 #include "ctprj.h"
+#include "ctprj_wavelet.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -39,6 +41,8 @@ extern "C" {
 #define CTPRJ_PROX_NONNEG 0   /* 'nonneg': x >= 0, no penalty */
 #define CTPRJ_PROX_TV_ISO 1   /* 'tviso': u TV_iso(x) + (x >= 0), TV.denoise(..., 'iso') */
 #define CTPRJ_PROX_TV_L1 2    /* 'tvl1':  u TV_l1(x) + (x >= 0), TV.denoise(..., 'l1') */
+#define CTPRJ_PROX_WVLT_ADMM 3  /* 'wvltADMM' (the reference's default): u |Psit(x)|_1 + (x >= 0),
+                                   admm(Psi, Psit, ...) of npg/admm.m, include/ctprj_wavelet.h */
 
 typedef struct {
     int iterations;             /* alternating iterations */
@@ -65,6 +69,9 @@ typedef struct {
     int no_adaptive_step;       /* 1: opt.adaptiveStep = false (no step growth after
                                    cumu_tol first-try successes) */
     int cumu_tol;               /* opt.cumuTol (<= 0: 4) */
+    int wvlt_filter_len;        /* CTPRJ_PROX_WVLT_ADMM: scaling filter length (<= 0: 2, Haar) */
+    double wvlt_filter[CTPRJ_WVLT_MAX_FILTER];   /* its taps, daubcqf(daub) (unused when <= 0) */
+    int wvlt_levels;            /* dwt_L (<= 0: 6, bhc/doBHC.m:33); n divisible by 2^dwt_L */
 } ctprj_bhc_loop_opts;
 
 typedef struct {

@@ -27,6 +27,7 @@ import numpy as np
 
 from . import bhc_oracle as BO
 from . import tv_oracle as TV
+from . import wavelet_oracle as WV
 
 
 def _cholesky_lifted(M, lift):
@@ -177,7 +178,7 @@ class _Density:
 def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, newton_steps=2,
                 method="npg", init_step="fixed", noise="poisson", skip_spectrum=False, thresh=0.0,
                 min_iterations=0, proximal="nonneg", u=0.0, max_inner=100, admm_tol=1e-2, restart=True,
-                adaptive_step=True, cumu_tol=4):
+                adaptive_step=True, cumu_tol=4, wvlt_h=None, wvlt_levels=6):
     """The alternating loop; forward(x) -> sinogram and backward(sino) -> image
     are FP64 projector callables.  Returns (x, Ie, stats) with stats holding
     the cost and accepted density step of every iteration.
@@ -190,7 +191,11 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
     or, when the inner iteration ran out, maxInnerItr * 10 (up to 1000) before
     x is kept (npg/NPG.m:99-134, npg/PG.m:97-121).  restart, adaptive_step,
     cumu_tol and admm_tol are the reference's opt.restart, opt.adaptiveStep,
-    opt.cumuTol and opt.admmTol (bhc/beamhardenSpline.m:277-294)."""
+    opt.cumuTol and opt.admmTol (bhc/beamhardenSpline.m:277-294).  proximal
+    "wvltADMM" (the reference's default) regularises with u |Psit(x)|_1: the
+    proximal map is admm(Psi, Psit, xbar - g/t, u/t, admmTol * difAlpha,
+    maxInnerItr, false, x) (npg/admm.m, wavelet_oracle.admm) with the wavelet
+    of scaling filter wvlt_h (default daubcqf(2)) and wvlt_levels levels."""
     dens = _Density(forward, backward, k, Ts, imea, noise)
     x = np.maximum(np.asarray(x, np.float64), 0.0)     # alpha = max(alpha, 0): :232, :236
     Ie = np.asarray(Ie, np.float64).copy()
@@ -212,10 +217,16 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
         if t == 0.0:
             t = np.finfo(np.float64).eps
     pg = method == "pg"
-    tv = proximal != "nonneg"
+    wv = proximal.lower() == "wvltadmm"
+    tv = proximal in ("tviso", "tvl1")
+    reg = tv or wv
     tvkind = "iso" if proximal == "tviso" else "l1"
     shape = x.shape if x.ndim == 2 else (int(round(math.sqrt(x.size))),) * 2
-    tlv = lambda v: TV.tlv(v.reshape(shape), tvkind) if tv else 0.0
+    wh = WV.daubcqf(2) if wvlt_h is None else np.asarray(wvlt_h, np.float64)
+    if wv:
+        tlv = lambda v: WV.l1_penalty(v.reshape(shape), wh, wvlt_levels)
+    else:
+        tlv = lambda v: TV.tlv(v.reshape(shape), tvkind) if tv else 0.0
     dif_alpha, pen = 1.0, 0.0
     inner = 0
     theta, cost, p, cumu = 0.0, math.inf, 0, 0
@@ -235,7 +246,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
         retries += 1
         return True
 
-    max_pass = 12 if tv else 3
+    max_pass = 12 if reg else 3
     for it in range(iterations):
         moved = False
         for pass_ in range(max_pass):
@@ -252,10 +263,14 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                 cumu, inc = 0, True
             while True:
                 ppp += 1
-                if tv:
+                if reg:
                     v = (xbar - g / t).reshape(shape)
-                    xn, inner = TV.tv_denoise(v, u / t, 0.0, math.inf, tvkind, max_inner,
-                                              admm_tol * dif_alpha)
+                    if tv:
+                        xn, inner = TV.tv_denoise(v, u / t, 0.0, math.inf, tvkind, max_inner,
+                                                  admm_tol * dif_alpha)
+                    else:
+                        xn, inner = WV.admm(v, u / t, wh, wvlt_levels, rel_tol=admm_tol * dif_alpha,
+                                            max_itr=max_inner, init=x.reshape(shape))
                     xn = xn.reshape(xbar.shape)
                     inner_total += inner
                 else:
@@ -281,7 +296,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
             moved = True
             if pg:
                 if not good_mm or new_obj > cost:
-                    if tv and not last and retry():
+                    if reg and not last and retry():
                         continue
                     moved = False
             elif new_obj > cost:
@@ -291,7 +306,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                 if not good_mm or f0 + u * tlv(xbar) < new_obj:
                     if not good_mm:
                         theta = 1.0
-                    if tv and not last and retry():
+                    if reg and not last and retry():
                         continue
                     moved = False
             if not moved:
@@ -300,7 +315,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
             xprev = x
             if moved:
                 x = xn
-            if tv:
+            if reg:
                 dif_alpha = float(np.linalg.norm(xprev - x)) / max(float(np.linalg.norm(x)), 1e-10)
             cumu = cumu + 1 if ppp == 1 and adaptive_step else 0
             break

@@ -143,3 +143,67 @@ def test_admm_zero_input_and_errors():
         wavelet.mdwt(x, np.ones(3), 1)                # odd filter
     with pytest.raises(CtprjError):
         wavelet.admm(x, -1.0, W.daubcqf(2), 2)        # negative weight
+
+
+def setup_problem(J=20, seed=4):
+    import oracle
+    from oracle import bhc_oracle as BO
+    from imgrecsrc_b200 import phantom
+    g = ct.Geometry(96, 136, 72, 72, 1.0, 1.0, 400.0)
+    Ts = 2.0 / g.n
+    x_true = phantom.two_material_phantom(g.n, seed=seed)
+    k = BO.kappa_nodes(J)
+    I_true = BO.spectrum_bump(J, seed)
+    s = Ts * oracle.forward(g, x_true.astype(np.float64))
+    BL, _, _ = BO.b1_iout(k, s.ravel(), I_true)
+    rng = np.random.default_rng(seed + 1)
+    m = (rng.poisson(1e5 * BL) / 1e5).reshape(g.np, g.prjWidth).astype(np.float32)
+    return g, Ts, x_true, k, I_true, m
+
+
+@pytest.mark.parametrize("method,daub", [("npg", 2), ("pg", 2), ("npg", 4)])
+def test_wvlt_loop_tracks_the_fp64_oracle_loop(method, daub):
+    """12 alternating iterations with the reference's default regulariser
+    ('wvltADMM', u = 1e-2, 5 levels): the GPU loop and the FP64 loop take the
+    same density steps and agree in cost, density and spectrum."""
+    import oracle
+    from oracle import bhc_loop_oracle as LO
+    from imgrecsrc_b200 import bhc
+    g, Ts, x_true, k, I_true, m = setup_problem()
+    h = W.daubcqf(daub)
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    dx = torch.full((g.n, g.n), 1.0, device="cuda")
+    dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
+    dm = torch.from_numpy(m).cuda()
+    st = model.reconstruct(dx, dI, dm, iterations=12, x_step=1e-3, method=method, proximal="wvltADMM", u=1e-2,
+                           wvlt_filter=h, wvlt_levels=5)
+    fw = lambda x: oracle.forward(g, x)
+    bw = lambda y: oracle.backward(g, y.reshape(g.np, g.prjWidth))
+    xo, Io, so = LO.reconstruct(fw, bw, k, Ts, np.ones((g.n, g.n)), np.full(20, 1.0 / 20),
+                                m.astype(np.float64), 12, x_step=1e-3, method=method, proximal="wvltADMM",
+                                u=1e-2, wvlt_h=h, wvlt_levels=5)
+    c, co = np.array(st["cost"]), np.array(so["cost"])
+    ex = rel(dx.cpu().numpy(), xo)
+    eI = rel(dI.cpu().numpy(), Io)
+    ec = float(np.max(np.abs(c - co) / np.abs(co)))
+    steps_equal = np.allclose(st["x_step"], so["x_step"], rtol=1e-12, atol=0)
+    print("wvlt loop vs FP64 oracle (%s, daub %d): max cost rel %.2e, x rel %.2e, Ie rel %.2e, same steps %s, "
+          "inner %d / %d, retries %d / %d" % (method, daub, ec, ex, eI, steps_equal, st["inner_iterations"],
+                                              so["inner_iterations"], st["prox_retries"], so["prox_retries"]))
+    assert steps_equal
+    assert ec < 1e-3
+    assert ex < 1e-3
+    assert eI < 1e-2
+    assert abs(st["inner_iterations"] - so["inner_iterations"]) <= 0.15 * so["inner_iterations"]
+    assert st["penalty"] > 0 and abs(st["penalty"] - so["penalty"]) / so["penalty"] < 1e-3
+
+
+def test_wvlt_loop_rejects_indivisible_image():
+    from imgrecsrc_b200 import bhc
+    g, Ts, x_true, k, I_true, m = setup_problem()
+    model = bhc.BHCModel(ct.Projector(g), k, Ts)
+    dx = torch.full((g.n, g.n), 1.0, device="cuda")
+    dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
+    with pytest.raises(CtprjError):   # 96 is not divisible by 2^6
+        model.reconstruct(dx, dI, torch.from_numpy(m).cuda(), iterations=2, proximal="wvltADMM", u=1e-2)
