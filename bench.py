@@ -449,7 +449,9 @@ def loop_leg(ct, g, pr, iters):
     FP64 non-negative spectrum step (Newton with an active-set QP on Ie >= 0),
     on the fused path and on the plain FP32 unfused path, then the same with
     the reference's default accelerated density step (npg/NPG.m), and NPG with
-    the isotropic TV proximal map (opt.proximal = 'tviso', u = 1e-3); iterations
+    the isotropic TV proximal map (opt.proximal = 'tviso') and with the
+    reference's default regulariser ('wvltADMM': Haar wavelet, 6 levels), both
+    at its default weight u = 1e-3; iterations
     per second, likelihood evaluations, spectrum time, and how far apart the
     fused and unfused results are."""
     import torch
@@ -472,7 +474,8 @@ def loop_leg(ct, g, pr, iters):
     res = {}
     for name, method, unfused, prox in (("pg_fused", "pg", False, "nonneg"), ("pg_unfused", "pg", True, "nonneg"),
                                         ("npg_fused", "npg", False, "nonneg"),
-                                        ("npg_tviso_fused", "npg", False, "tviso")):
+                                        ("npg_tviso_fused", "npg", False, "tviso"),
+                                        ("npg_wvlt_fused", "npg", False, "wvltADMM")):
         x = torch.full((g.n, g.n), 1.0, device="cuda")
         Ie = torch.full((J,), 1.0 / J, dtype=torch.float64, device="cuda")
         st = model.reconstruct(x, Ie, imea, iterations=iters, x_step=1e-3, unfused=unfused, method=method,
@@ -625,6 +628,28 @@ def extras_leg(ct, g, pr, flush, stream, steps):
     out["tv_denoise"] = {"workload": "isotropic TV FGP on %d^2, lambda 0.05, %d iterations" % (g.n, tv_iters),
                          "ms": tv_ms, "ms_20_iterations": tv_ms20, "us_per_iteration": us_it,
                          "algorithmic_GBps": 36.0 * g.n * g.n / (us_it * 1e-6) / 1e9}
+    # the wavelet ADMM proximal map (npg/admm.m, Haar, 6 levels) on the headline
+    # image size: marginal time of 80 more iterations (relativeTol = 0).
+    # Algorithmic bytes per iteration, per pixel: the inverse transform reads
+    # s and nu (8 B) and a (4 B) and writes alpha (4 B); the forward transform
+    # reads alpha (4 B) and its epilogue reads nu, s_old and writes nu, s_new
+    # (16 B); the LL blocks of the coarser levels add 4/3 (4 + 4) B each way
+    from imgrecsrc_b200 import wavelet as wvm
+    haar = np.ascontiguousarray(wvm.daubcqf(2))
+    wa = torch.rand(g.n, g.n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(11)) - 0.3
+    wo = torch.empty_like(wa)
+
+    def admm_run(iters):
+        ct.check(L.ctprj_wvlt_admm(vp(wa), g.n, g.n, haar.ctypes.data, 2, 6, 0.05, 0.0, iters, None, vp(wo),
+                                   ctypes.byref(itn), hs))
+    wv_ms = timed(lambda: admm_run(100))
+    wv_ms20 = timed(lambda: admm_run(20))
+    wv_us = 1e3 * (wv_ms - wv_ms20) / 80
+    wv_bytes = (8 + 4 + 4 + 4 + 16 + 2 * (4.0 / 3.0) * 4) * g.n * g.n
+    out["wvlt_admm"] = {"workload": "wavelet ADMM (Haar, 6 levels, u 0.05) on %d^2, 101 iterations" % g.n,
+                        "ms": wv_ms, "ms_21_iterations": wv_ms20, "us_per_iteration": wv_us,
+                        "algorithmic_GBps": wv_bytes / (wv_us * 1e-6) / 1e9,
+                        "launches_per_iteration": 2 * 6 + 1}
     out["parprj"] = {"workload": "FP64 masked parallel operator (mParPrj): %d^2 image, disc mask of %d "
                                  "pixels, %d angles over [0,180) deg, %d detectors" % (n, mask.size, nang, W),
                      "forward_ms": timed(fwd), "backward_ms": timed(bwd)}
