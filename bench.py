@@ -629,11 +629,10 @@ def extras_leg(ct, g, pr, flush, stream, steps):
                          "ms": tv_ms, "ms_20_iterations": tv_ms20, "us_per_iteration": us_it,
                          "algorithmic_GBps": 36.0 * g.n * g.n / (us_it * 1e-6) / 1e9}
     # the wavelet ADMM proximal map (npg/admm.m, Haar, 6 levels) on the headline
-    # image size: marginal time of 80 more iterations (relativeTol = 0).
-    # Algorithmic bytes per iteration, per pixel: the inverse transform reads
-    # s and nu (8 B) and a (4 B) and writes alpha (4 B); the forward transform
-    # reads alpha (4 B) and its epilogue reads nu, s_old and writes nu, s_new
-    # (16 B); the LL blocks of the coarser levels add 4/3 (4 + 4) B each way
+    # image size: marginal time of 80 more iterations (relativeTol = 0), by the
+    # fused per-tile iteration (one launch: s, nu and a in, s and nu out, 20 B
+    # per pixel) and, for comparison, by the level-by-level passes
+    # (CTPRJ_WVLT_KERNEL=levels: 13 launches, about 41 B per pixel)
     from imgrecsrc_b200 import wavelet as wvm
     haar = np.ascontiguousarray(wvm.daubcqf(2))
     wa = torch.rand(g.n, g.n, device="cuda", generator=torch.Generator(device="cuda").manual_seed(11)) - 0.3
@@ -642,14 +641,23 @@ def extras_leg(ct, g, pr, flush, stream, steps):
     def admm_run(iters):
         ct.check(L.ctprj_wvlt_admm(vp(wa), g.n, g.n, haar.ctypes.data, 2, 6, 0.05, 0.0, iters, None, vp(wo),
                                    ctypes.byref(itn), hs))
-    wv_ms = timed(lambda: admm_run(100))
-    wv_ms20 = timed(lambda: admm_run(20))
-    wv_us = 1e3 * (wv_ms - wv_ms20) / 80
-    wv_bytes = (8 + 4 + 4 + 4 + 16 + 2 * (4.0 / 3.0) * 4) * g.n * g.n
+
+    def admm_us():
+        t100, t20 = timed(lambda: admm_run(100)), timed(lambda: admm_run(20))
+        return t100, 1e3 * (t100 - t20) / 80
+    wv_ms, wv_us = admm_us()
+    os.environ["CTPRJ_WVLT_KERNEL"] = "levels"
+    try:
+        wl_ms, wl_us = admm_us()
+    finally:
+        del os.environ["CTPRJ_WVLT_KERNEL"]
     out["wvlt_admm"] = {"workload": "wavelet ADMM (Haar, 6 levels, u 0.05) on %d^2, 101 iterations" % g.n,
-                        "ms": wv_ms, "ms_21_iterations": wv_ms20, "us_per_iteration": wv_us,
-                        "algorithmic_GBps": wv_bytes / (wv_us * 1e-6) / 1e9,
-                        "launches_per_iteration": 2 * 6 + 1}
+                        "ms": wv_ms, "us_per_iteration": wv_us,
+                        "algorithmic_GBps": 20.0 * g.n * g.n / (wv_us * 1e-6) / 1e9,
+                        "launches_per_iteration": 1,
+                        "level_passes": {"ms": wl_ms, "us_per_iteration": wl_us, "launches_per_iteration": 13,
+                                         "algorithmic_GBps": (8 + 4 + 4 + 4 + 16 + 2 * (4.0 / 3.0) * 4)
+                                         * g.n * g.n / (wl_us * 1e-6) / 1e9}}
     out["parprj"] = {"workload": "FP64 masked parallel operator (mParPrj): %d^2 image, disc mask of %d "
                                  "pixels, %d angles over [0,180) deg, %d detectors" % (n, mask.size, nang, W),
                      "forward_ms": timed(fwd), "backward_ms": timed(bwd)}

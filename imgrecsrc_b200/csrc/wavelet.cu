@@ -26,6 +26,8 @@
 // doubling / halving of nu that accompanies a rho change is applied as a
 // factor when nu is next read.
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "ctprj_internal.h"
@@ -50,6 +52,7 @@ struct AdmmState {
     int cnt;          // iterations since the last rho change
     int done;
     int max_itr;
+    unsigned arrived; // blocks of the running fused iteration that have written their partials
 };
 
 enum { kEpiStore = 0, kEpiAdmm = 1, kEpiL1 = 2 };
@@ -233,29 +236,12 @@ __global__ void __launch_bounds__(kWvThreads) k_wvlt_synthesis(const SynArgs a)
         }
 }
 
-// the iteration's scalars (npg/admm.m's loop tail): the stopping rule, then
-// the rho adaptation after more than 20 iterations without one
-__global__ void __launch_bounds__(256) k_admm_scalars(AdmmState *st, const double *__restrict__ part, int nblocks)
+// the iteration's scalars (npg/admm.m's loop tail) from the sums of
+// |s - s_old|^2 and |s - Psit(alpha)|^2: the stopping rule, then the rho
+// adaptation after more than 20 iterations without one
+__device__ void admm_advance(AdmmState *st, double dif2, double res2)
 {
-    __shared__ double red[2][256];
-    if (st->done) return;
-    double s0 = 0.0, s1 = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += 256) {
-        s0 += part[2 * (size_t)b];
-        s1 += part[2 * (size_t)b + 1];
-    }
-    red[0][threadIdx.x] = s0;
-    red[1][threadIdx.x] = s1;
-    __syncthreads();
-    for (int h = 128; h > 0; h >>= 1) {
-        if ((int)threadIdx.x < h) {
-            red[0][threadIdx.x] += red[0][threadIdx.x + h];
-            red[1][threadIdx.x] += red[1][threadIdx.x + h];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x != 0) return;
-    const double dif = sqrt(red[0][0]), res = sqrt(red[1][0]);
+    const double dif = sqrt(dif2), res = sqrt(res2);
     st->dif = dif;
     st->res = res;
     st->iter += 1;
@@ -278,6 +264,28 @@ __global__ void __launch_bounds__(256) k_admm_scalars(AdmmState *st, const doubl
     }
 }
 
+__global__ void __launch_bounds__(256) k_admm_scalars(AdmmState *st, const double *__restrict__ part, int nblocks)
+{
+    __shared__ double red[2][256];
+    if (st->done) return;
+    double s0 = 0.0, s1 = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += 256) {
+        s0 += part[2 * (size_t)b];
+        s1 += part[2 * (size_t)b + 1];
+    }
+    red[0][threadIdx.x] = s0;
+    red[1][threadIdx.x] = s1;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + h];
+            red[1][threadIdx.x] += red[1][threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) admm_advance(st, red[0][0], red[1][0]);
+}
+
 __global__ void k_admm_start(AdmmState *st, double tol, int max_itr)
 {
     st->rho = 1.0;
@@ -288,6 +296,237 @@ __global__ void k_admm_start(AdmmState *st, double tol, int max_itr)
     st->cnt = 0;
     st->done = 0;
     st->max_itr = max_itr;
+    st->arrived = 0;
+}
+
+// ---- two-tap filters: one fused launch per ADMM iteration ----------------
+// With a 2-tap filter every level reads only its own 2 x 2 input cells, so a
+// 2^L x 2^L image tile holds every coefficient of all L levels that it
+// touches and needs nothing from its neighbours.  One block per tile then
+// does a whole iteration in shared memory: gather s + nu_mul nu from the
+// tile's coefficient positions (Mallat order inside the tile), the inverse
+// transform coarsest level first, alpha = max((a + rho x) / (1 + rho), 0),
+// the forward transform finest level first, and the ADMM update written back
+// to the same positions -- 20 bytes per pixel (s, nu, a in; s, nu out) and no
+// alpha image.  Each level works in place: a thread reads its cells into
+// registers, the block synchronises, then writes.  The arithmetic is the
+// level kernels' operation for operation; only the FP64 partial sums are
+// added in another order.  The last block to finish sums every tile's
+// partials in a fixed order and advances the scalars.
+constexpr int kHaarMaxLevels = 6;
+constexpr int kHaarThreads = 256;
+
+struct HaarArgs {
+    float h0, h1, g0, g1;
+    int rows, cols;
+    const float *a;
+    float *s0, *s1, *nu;
+    float *alpha;             // the final pass writes alpha here
+    AdmmState *st;
+    double u;
+    double *part;             // per-tile partials, 2 each
+    int final_pass;
+};
+
+// coefficient-array index of tile-layout cell (r, c) of tile (ti, tj)
+template <int L>
+__device__ __forceinline__ int haar_coef_index(int r, int c, int ti, int tj, int rows, int cols)
+{
+    const int m = r | c;   // its highest bit is that of max(r, c)
+    int lev = L, Tl = 1, qr = 0, qc = 0;
+    if (m) {
+        const int b = 31 - __clz(m);
+        Tl = 1 << b;
+        lev = L - b;
+        qr = r >= Tl;
+        qc = c >= Tl;
+    }
+    const int grow = ti * Tl + (r - qr * Tl) + qr * (rows >> lev);
+    const int gcol = tj * Tl + (c - qc * Tl) + qc * (cols >> lev);
+    return grow * cols + gcol;
+}
+
+template <int L>
+__global__ void __launch_bounds__(kHaarThreads) k_admm_haar(const HaarArgs a)
+{
+    constexpr int T = 1 << L, P = T + 1;
+    constexpr int kItems = ((T / 2) * (T / 2) + kHaarThreads - 1) / kHaarThreads;
+    extern __shared__ float sm[];
+    float *W = sm;              // working tile, T x P
+    float *Sv = sm + T * P;     // s_old, tile layout
+    float *Nv = Sv + T * T;     // stored nu, tile layout
+    __shared__ bool last;
+    AdmmState *st = a.st;
+    if (!a.final_pass && st->done) return;
+    const int t = threadIdx.x, ti = blockIdx.y, tj = blockIdx.x;
+    const int cur = st->iter & 1;
+    const float *Sc = cur ? a.s1 : a.s0;
+    float *Sn = cur ? a.s0 : a.s1;
+    const float mul = (float)st->nu_mul, rho = (float)st->rho, thr = (float)(a.u / st->rho);
+    const float h0 = a.h0, h1 = a.h1, g0 = a.g0, g1 = a.g1;
+    for (int idx = t; idx < T * T; idx += kHaarThreads) {
+        const int r = idx >> L, c = idx & (T - 1);
+        const int gp = haar_coef_index<L>(r, c, ti, tj, a.rows, a.cols);
+        const float sv = Sc[gp], nv = a.nu[gp];
+        W[r * P + c] = fmaf(mul, nv, sv);
+        Sv[idx] = sv;
+        Nv[idx] = nv;
+    }
+    __syncthreads();
+    // inverse transform, coarsest level first
+    for (int lev = L; lev >= 1; --lev) {
+        const int Tl = T >> lev, n = Tl * Tl;
+        float c00[kItems], c01[kItems], c10[kItems], c11[kItems];
+#pragma unroll
+        for (int it = 0; it < kItems; ++it) {
+            const int q = t + it * kHaarThreads;
+            if (q < n) {
+                const int kk = q / Tl, ll = q % Tl;
+                c00[it] = W[kk * P + ll];
+                c01[it] = W[kk * P + ll + Tl];
+                c10[it] = W[(kk + Tl) * P + ll];
+                c11[it] = W[(kk + Tl) * P + ll + Tl];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < kItems; ++it) {
+            const int q = t + it * kHaarThreads;
+            if (q < n) {
+                const int kk = q / Tl, ll = q % Tl;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const float he = e ? h1 : h0, ge = e ? g1 : g0;
+                    const float ulo = fmaf(he, c00[it], fmaf(ge, c10[it], 0.0f));
+                    const float uhi = fmaf(he, c01[it], fmaf(ge, c11[it], 0.0f));
+                    W[(2 * kk + e) * P + 2 * ll] = fmaf(h0, ulo, fmaf(g0, uhi, 0.0f));
+                    W[(2 * kk + e) * P + 2 * ll + 1] = fmaf(h1, ulo, fmaf(g1, uhi, 0.0f));
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // alpha = max((a + rho x) / (1 + rho), 0)
+    for (int idx = t; idx < T * T; idx += kHaarThreads) {
+        const int r = idx >> L, c = idx & (T - 1);
+        const size_t gpix = (size_t)(ti * T + r) * a.cols + tj * T + c;
+        const float v = fmaxf(fmaf(rho, W[r * P + c], a.a[gpix]) / (1.0f + rho), 0.0f);
+        if (a.final_pass)
+            a.alpha[gpix] = v;
+        else
+            W[r * P + c] = v;
+    }
+    if (a.final_pass) return;
+    __syncthreads();
+    // forward transform, finest level first
+    for (int lev = 1; lev <= L; ++lev) {
+        const int Tl = T >> lev, n = Tl * Tl;
+        float x00[kItems], x01[kItems], x10[kItems], x11[kItems];
+#pragma unroll
+        for (int it = 0; it < kItems; ++it) {
+            const int q = t + it * kHaarThreads;
+            if (q < n) {
+                const int kk = q / Tl, ll = q % Tl;
+                x00[it] = W[2 * kk * P + 2 * ll];
+                x01[it] = W[2 * kk * P + 2 * ll + 1];
+                x10[it] = W[(2 * kk + 1) * P + 2 * ll];
+                x11[it] = W[(2 * kk + 1) * P + 2 * ll + 1];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < kItems; ++it) {
+            const int q = t + it * kHaarThreads;
+            if (q < n) {
+                const int kk = q / Tl, ll = q % Tl;
+                const float lo0 = fmaf(h1, x01[it], fmaf(h0, x00[it], 0.0f));
+                const float hi0 = fmaf(g1, x01[it], fmaf(g0, x00[it], 0.0f));
+                const float lo1 = fmaf(h1, x11[it], fmaf(h0, x10[it], 0.0f));
+                const float hi1 = fmaf(g1, x11[it], fmaf(g0, x10[it], 0.0f));
+                W[kk * P + ll] = fmaf(h1, lo1, fmaf(h0, lo0, 0.0f));
+                W[kk * P + ll + Tl] = fmaf(h1, hi1, fmaf(h0, hi0, 0.0f));
+                W[(kk + Tl) * P + ll] = fmaf(g1, lo1, fmaf(g0, lo0, 0.0f));
+                W[(kk + Tl) * P + ll + Tl] = fmaf(g1, hi1, fmaf(g0, hi0, 0.0f));
+            }
+        }
+        __syncthreads();
+    }
+    // s = soft(v - nu, u / rho), nu = nu + s - v at every coefficient of the tile
+    double p0 = 0.0, p1 = 0.0;
+    for (int idx = t; idx < T * T; idx += kHaarThreads) {
+        const int r = idx >> L, c = idx & (T - 1);
+        const int gp = haar_coef_index<L>(r, c, ti, tj, a.rows, a.cols);
+        const float v = W[r * P + c];
+        const float nue = mul * Nv[idx];
+        const float w = v - nue;
+        const float sn = w > thr ? w - thr : (w < -thr ? w + thr : 0.0f);
+        a.nu[gp] = nue + sn - v;
+        Sn[gp] = sn;
+        const double d = (double)sn - (double)Sv[idx], rr = (double)sn - (double)v;
+        p0 = fma(d, d, p0);
+        p1 = fma(rr, rr, p1);
+    }
+    double out[2];
+    block_sum2(p0, p1, out);
+    const unsigned nblocks = gridDim.x * gridDim.y;
+    if (t == 0) {
+        const size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+        a.part[2 * b] = out[0];
+        a.part[2 * b + 1] = out[1];
+        __threadfence();
+        last = atomicAdd(&st->arrived, 1u) == nblocks - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    // the last block: every tile's partials in a fixed order, then the scalars
+    __threadfence();
+    __shared__ double red[2][kHaarThreads];
+    double q0 = 0.0, q1 = 0.0;
+    for (unsigned b = t; b < nblocks; b += kHaarThreads) {
+        q0 += __ldcg(a.part + 2 * (size_t)b);
+        q1 += __ldcg(a.part + 2 * (size_t)b + 1);
+    }
+    red[0][t] = q0;
+    red[1][t] = q1;
+    __syncthreads();
+    for (int h = kHaarThreads / 2; h > 0; h >>= 1) {
+        if (t < h) {
+            red[0][t] += red[0][t + h];
+            red[1][t] += red[1][t + h];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        admm_advance(st, red[0][0], red[1][0]);
+        st->arrived = 0;
+    }
+}
+
+template <int L>
+int launch_admm_haar_t(const HaarArgs &a, cudaStream_t s)
+{
+    constexpr int T = 1 << L;
+    const size_t smem = sizeof(float) * ((size_t)T * (T + 1) + 2 * (size_t)T * T);
+    int st;
+    if ((st = cuda_error(cudaFuncSetAttribute(k_admm_haar<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                         "ADMM shared memory")))
+        return st;
+    const dim3 grid((unsigned)(a.cols / T), (unsigned)(a.rows / T));
+    k_admm_haar<L><<<grid, kHaarThreads, smem, s>>>(a);
+    return cuda_error(cudaGetLastError(), "ADMM iteration");
+}
+
+int launch_admm_haar(int levels, const HaarArgs &a, cudaStream_t s)
+{
+    switch (levels) {
+    case 1: return launch_admm_haar_t<1>(a, s);
+    case 2: return launch_admm_haar_t<2>(a, s);
+    case 3: return launch_admm_haar_t<3>(a, s);
+    case 4: return launch_admm_haar_t<4>(a, s);
+    case 5: return launch_admm_haar_t<5>(a, s);
+    case 6: return launch_admm_haar_t<6>(a, s);
+    default: return set_error(CTPRJ_EINVAL, "fused ADMM: at most %d levels", kHaarMaxLevels);
+    }
 }
 
 __global__ void __launch_bounds__(256) k_wvlt_sumsq(const float *__restrict__ x, long long n, double *__restrict__ part)
@@ -492,13 +731,37 @@ int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h,
         return st;
     k_admm_start<<<1, 1, 0, s>>>(dst, tol, max_itr);
     const int nblocks = analysis_blocks(rows, cols, levels);
+    // two-tap filters up to kHaarMaxLevels levels: the fused per-tile iteration
+    // (CTPRJ_WVLT_KERNEL=levels keeps the level-by-level passes, for comparison)
+    const char *kenv = getenv("CTPRJ_WVLT_KERNEL");
+    const bool fused = lh == 2 && levels <= kHaarMaxLevels && !(kenv && !strcmp(kenv, "levels"));
+    HaarArgs ha;
+    ha.h0 = f.h[0];
+    ha.h1 = f.h[1];
+    ha.g0 = f.g[0];
+    ha.g1 = f.g[1];
+    ha.rows = rows;
+    ha.cols = cols;
+    ha.a = a;
+    ha.s0 = s0;
+    ha.s1 = s1;
+    ha.nu = nu;
+    ha.alpha = alpha;
+    ha.st = dst;
+    ha.u = u;
+    ha.part = ws.part;
+    ha.final_pass = 0;
     AdmmState h_st{};
     for (int it = 0; it <= max_itr + 1; ++it) {
-        if ((st = run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 0, a, alpha, s)) ||
-            (st = run_analysis(f, alpha, rows, cols, levels, scratch, kEpiAdmm, nullptr, dst, s0, s1, nu, u,
-                               ws.part, s)))
-            return st;
-        k_admm_scalars<<<1, 256, 0, s>>>(dst, ws.part, nblocks);
+        if (fused) {
+            if ((st = launch_admm_haar(levels, ha, s))) return st;
+        } else {
+            if ((st = run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 0, a, alpha, s)) ||
+                (st = run_analysis(f, alpha, rows, cols, levels, scratch, kEpiAdmm, nullptr, dst, s0, s1, nu, u,
+                                   ws.part, s)))
+                return st;
+            k_admm_scalars<<<1, 256, 0, s>>>(dst, ws.part, nblocks);
+        }
         if ((st = cuda_error(cudaGetLastError(), "ADMM iteration"))) return st;
         if ((it & 7) == 7) {
             if ((st = cuda_error(cudaMemcpyAsync(&h_st, dst, sizeof h_st, cudaMemcpyDeviceToHost, s), "ADMM state")) ||
@@ -508,7 +771,9 @@ int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h,
         }
     }
     // alpha = max((a + rho Psi(s + nu)) / (1 + rho), 0) from the last s, nu
-    if ((st = run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 1, a, alpha, s)) ||
+    ha.final_pass = 1;
+    if ((st = fused ? launch_admm_haar(levels, ha, s)
+                    : run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 1, a, alpha, s)) ||
         (st = cuda_error(cudaMemcpyAsync(&h_st, dst, sizeof h_st, cudaMemcpyDeviceToHost, s), "ADMM state")) ||
         (st = cuda_error(cudaStreamSynchronize(s), "ADMM state")))
         return st;

@@ -132,6 +132,31 @@ def test_admm_stopping_rule_and_objective():
         assert abs(f - fo) / fo < 1e-5
 
 
+@pytest.mark.parametrize("L,shape", [(6, (256, 192)), (3, (40, 64)), (1, (6, 10))])
+def test_fused_two_tap_iteration_matches_the_level_passes(L, shape, monkeypatch):
+    """The fused per-tile iteration (two-tap filters, up to 6 levels) against
+    the level-by-level passes (CTPRJ_WVLT_KERNEL=levels) and the FP64
+    restatement: the same arithmetic, so the same iterations and alpha to
+    rounding of the FP64 partial sums' order."""
+    rng = np.random.default_rng(L)
+    a = rng.standard_normal(shape) + 0.3
+    init = np.maximum(rng.standard_normal(shape), 0.0)
+    h = W.daubcqf(2)
+    fa, it_f = wavelet.admm(dev(a), 0.4, h, L, relative_tol=0.0, max_itr=45, init=dev(init))
+    monkeypatch.setenv("CTPRJ_WVLT_KERNEL", "levels")
+    la, it_l = wavelet.admm(dev(a), 0.4, h, L, relative_tol=0.0, max_itr=45, init=dev(init))
+    monkeypatch.delenv("CTPRJ_WVLT_KERNEL")
+    alo, ito = W.admm(a.astype(np.float32).astype(np.float64), 0.4, h, L, rel_tol=0.0, max_itr=45,
+                      init=init.astype(np.float32).astype(np.float64))
+    e_fl = rel(fa.cpu().numpy(), la.cpu().numpy())
+    e_fo = rel(fa.cpu().numpy(), alo)
+    print("fused vs levels (L %d, %s): %d / %d / %d iterations, rel %.2e, vs FP64 %.2e" % (
+        L, shape, it_f, it_l, ito, e_fl, e_fo))
+    assert it_f == it_l == ito == 46
+    assert e_fl < 1e-6
+    assert e_fo < 1e-4
+
+
 def test_admm_zero_input_and_errors():
     z = torch.zeros(32, 32, device="cuda")
     out, it = wavelet.admm(z, 0.1, W.daubcqf(2), 3)
