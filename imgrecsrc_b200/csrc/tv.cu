@@ -26,6 +26,7 @@
 // (count, restart, t, the momentum coefficient, done), so every decision
 // stays on the device; the host checks the done flag every eight
 // iterations, and launches after convergence change nothing.
+#include <algorithm>
 #include <cmath>
 
 #include "ctprj_internal.h"
@@ -102,18 +103,114 @@ __device__ void tv_advance(TvState *st, const double s[4], int max_iter, double 
     if (st->count >= 5 || st->iter >= max_iter) st->done = 1;
 }
 
-// One FGP iteration on a kTvTile x kTvTile tile.  Thread (tx, ty) of the
-// 32 x 8 block owns column j0 + tx of rows ty, ty + 8, ty + 16, ty + 24, so
-// every warp reads and writes whole rows; all global loads of the iteration
-// (P, P_prev as float2 pairs, Xobs, D_old) are issued before the first
-// barrier.  The last block to finish sums every block's partials in a fixed
-// order and advances the scalars, so an iteration is one launch.
-__global__ void __launch_bounds__(kTvThreads, 4) k_tv_iter(const TvArgs a)
+// cp.async copies of 8 or 4 bytes into shared memory; src_size 0 (a tile cell
+// outside the image) writes zeros and reads nothing
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem, bool valid)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid ? 4 : 0));
+}
+// 16 bytes, the first `bytes` of them read (the rest zero); both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// Shared-memory stage of one tile: P and P_prev on rows i0-1 .. i0+T and
+// columns j0-2 .. j0+T+1 (float2 pairs; the extra column on each side keeps
+// the 16-byte copies aligned), Xobs on rows i0 .. i0+T and columns
+// j0 .. j0+T+3, D_old on the tile.  Cells outside the image are zero, which is
+// what P, the difference operators and the clamped reads need there.
+constexpr int kTvPR = kTvTile + 2, kTvPW = kTvTile + 4, kTvXR = kTvTile + 1, kTvXW = kTvTile + 4;
+struct TvStage {
+    float2 P[kTvPR][kTvPW];
+    float2 Q[kTvPR][kTvPW];
+    float X[kTvXR][kTvXW];
+    float D[kTvTile][kTvTile];
+};
+struct TvSmem {
+    TvStage st[2];
+    float R1s[kTvTile + 2][kTvTile + 1];   // rows i0-1 .. i0+T, cols j0 .. j0+T
+    float R2s[kTvTile + 1][kTvTile + 2];   // rows i0 .. i0+T, cols j0-1 .. j0+T
+    float Ds[kTvTile + 1][kTvTile + 1];    // rows i0 .. i0+T, cols j0 .. j0+T
+};
+
+// 16-byte copies (two dual pairs or four floats) when a row starts 16-byte
+// aligned (cols % 4 == 0), else 8- / 4-byte copies
+template <bool VEC>
+__device__ __forceinline__ void tv_stage_load(TvStage &S, const TvArgs &a, const float2 *P, const float2 *Q,
+                                              const float *Dold, int i0, int j0, int t)
 {
     constexpr int T = kTvTile;
-    __shared__ float R1s[T + 2][T + 1];   // rows i0-1 .. i0+T, cols j0 .. j0+T
-    __shared__ float R2s[T + 1][T + 2];   // rows i0 .. i0+T, cols j0-1 .. j0+T
-    __shared__ float Ds[T + 1][T + 1];    // rows i0 .. i0+T, cols j0 .. j0+T
+    const int m = a.m, n = a.n;
+    if (VEC) {
+        for (int e = t; e < kTvPR * (kTvPW / 2); e += kTvThreads) {   // pairs of float2
+            const int r = e / (kTvPW / 2), c = 2 * (e % (kTvPW / 2));
+            const int i = i0 - 1 + r, j = j0 - 2 + c;
+            const int cnt = (i >= 0 && i < m && j >= 0) ? max(0, min(2, n - j)) : 0;
+            const int q = cnt ? i * n + j : 0;
+            cp_async16(&S.P[r][c], P + q, 8 * cnt);
+            cp_async16(&S.Q[r][c], Q + q, 8 * cnt);
+        }
+        for (int e = t; e < kTvXR * (kTvXW / 4); e += kTvThreads) {   // quads of floats
+            const int r = e / (kTvXW / 4), c = 4 * (e % (kTvXW / 4));
+            const int i = i0 + r, j = j0 + c;
+            const int cnt = i < m ? max(0, min(4, n - j)) : 0;
+            cp_async16(&S.X[r][c], a.xobs + (cnt ? i * n + j : 0), 4 * cnt);
+        }
+        for (int e = t; e < T * (T / 4); e += kTvThreads) {
+            const int r = e / (T / 4), c = 4 * (e % (T / 4));
+            const int i = i0 + r, j = j0 + c;
+            const int cnt = i < m ? max(0, min(4, n - j)) : 0;
+            cp_async16(&S.D[r][c], Dold + (cnt ? i * n + j : 0), 4 * cnt);
+        }
+        return;
+    }
+    for (int e = t; e < kTvPR * kTvPW; e += kTvThreads) {
+        const int r = e / kTvPW, c = e % kTvPW;
+        const int i = i0 - 1 + r, j = j0 - 2 + c;
+        const bool v = i >= 0 && i < m && j >= 0 && j < n;
+        const int q = v ? i * n + j : 0;
+        cp_async8(&S.P[r][c], P + q, v);
+        cp_async8(&S.Q[r][c], Q + q, v);
+    }
+    for (int e = t; e < kTvXR * kTvXW; e += kTvThreads) {
+        const int r = e / kTvXW, c = e % kTvXW;
+        const int i = i0 + r, j = j0 + c;
+        const bool v = i < m && j < n;
+        cp_async4(&S.X[r][c], a.xobs + (v ? i * n + j : 0), v);
+    }
+    for (int e = t; e < T * T; e += kTvThreads) {
+        const int r = e / T, c = e % T;
+        const int i = i0 + r, j = j0 + c;
+        const bool v = i < m && j < n;
+        cp_async4(&S.D[r][c], Dold + (v ? i * n + j : 0), v);
+    }
+}
+
+// One FGP iteration.  Persistent blocks step through the kTvTile x kTvTile
+// tiles; while a block computes one tile from a shared-memory stage, cp.async
+// streams its next tile into the other stage, so the memory system stays
+// busy across the compute phases.  Per tile: R = P + c (P - P_prev) on the
+// tile and a one-pixel halo, C = Xobs - lambda L(R) and D = clamp(C) on the
+// tile plus its bottom row and right column, then the new P on the tile.
+// Thread (tx, ty) of the 32 x 8 block owns column tx of rows ty, ty + 8, ...
+// The last block to finish sums every block's partials in a fixed order and
+// advances the scalars, so an iteration is one launch.
+template <bool VEC>
+__global__ void __launch_bounds__(kTvThreads) k_tv_iter(const TvArgs a, int tiles_x, int ntiles)
+{
+    constexpr int T = kTvTile;
+    extern __shared__ __align__(16) unsigned char tv_smem[];
+    TvSmem &S = *reinterpret_cast<TvSmem *>(tv_smem);
     __shared__ bool last;
     TvState *st = a.st;
     if (st->done) return;
@@ -125,108 +222,86 @@ __global__ void __launch_bounds__(kTvThreads, 4) k_tv_iter(const TvArgs a)
     float2 *N = tv_p(a.buf, a.px, (it + 1) % 3);          // new P
     const float *Dold = tv_d(a.buf, a.px, it & 1);
     float *Dn = tv_d(a.buf, a.px, (it + 1) & 1);
-    const int i0 = blockIdx.y * T, j0 = blockIdx.x * T;
     const int tx = threadIdx.x, ty = threadIdx.y, t = ty * 32 + tx;
-    const int j = j0 + tx;
-    // R = P + c (P - P_prev) on rows i0-1 .. i0+T.  R1 (vertical
-    // differences) exists for rows < m-1, R2 for columns < n-1; elsewhere it
-    // is 0, which makes L(R) one formula everywhere.  Every load reads a
-    // clamped, valid address and is masked afterwards, so none waits behind a
-    // bounds branch.
-    const int jc = min(j, n - 1);
-    float2 pv[5], qv[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        const int q = min(max(i0 - 1 + ty + 8 * k, 0), m - 1) * n + jc;   // m * n < 2^31
-        pv[k] = P[q];
-        qv[k] = Q[q];
-    }
-    // halo columns: j0 + T (R1 and R2, rows i0-1 .. i0+T) and j0 - 1 (R2)
-    const int hr = t % (T + 2), hside = t / (T + 2);
-    const int hI = i0 - 1 + hr, hJ = hside ? j0 - 1 : j0 + T;
-    const int qh = min(max(hI, 0), m - 1) * n + min(max(hJ, 0), n - 1);
-    const float2 hp = P[qh], hq = Q[qh];
-    float xo[4], dol[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int q = min(i0 + ty + 8 * k, m - 1) * n + jc;
-        xo[k] = a.xobs[q];
-        dol[k] = Dold[q];
-    }
-    // Xobs of the halo D: the bottom row (warp 0), the right column (warp 1)
-    const int hi = ty == 0 ? i0 + T : i0 + tx, hj = ty == 0 ? j : j0 + T;
-    const bool hin = ty < 2 && hi < m && hj < n;
-    const float xh = a.xobs[min(hi, m - 1) * n + min(hj, n - 1)];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        const int r = ty + 8 * k, i = i0 - 1 + r;      // R1s row r, R2s row r - 1
-        if (r < T + 2) {
-            R1s[r][tx] = (i >= 0 && i < m - 1 && j < n) ? fmaf(c, pv[k].x - qv[k].x, pv[k].x) : 0.0f;
-            if (r >= 1)
-                R2s[r - 1][tx + 1] = (i < m && j < n - 1) ? fmaf(c, pv[k].y - qv[k].y, pv[k].y) : 0.0f;
-        }
-    }
-    if (hside == 0 && hr < T + 2) {       // column j0 + T
-        R1s[hr][T] = (hI >= 0 && hI < m - 1 && hJ < n) ? fmaf(c, hp.x - hq.x, hp.x) : 0.0f;
-        if (hr >= 1) R2s[hr - 1][T + 1] = (hI < m && hJ < n - 1) ? fmaf(c, hp.y - hq.y, hp.y) : 0.0f;
-    } else if (hside == 1 && hr >= 1) {   // column j0 - 1
-        R2s[hr - 1][0] = (hI < m && hJ >= 0 && hJ < n - 1) ? fmaf(c, hp.y - hq.y, hp.y) : 0.0f;
-    }
-    __syncthreads();
-    // C = Xobs - lambda L(R), D = clamp(C) on the tile (partials) and halo
-    const float lam = a.lam, lb = a.lb, ub = a.ub;
+    const float lam = a.lam, lb = a.lb, ub = a.ub, inv8l = 1.0f / (8.0f * lam);
     double s[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int r = ty + 8 * k, i = i0 + r;
-        if (i < m && j < n) {
-            const float L = (R1s[r + 1][tx] - R1s[r][tx]) + (R2s[r][tx + 1] - R2s[r][tx]);
-            const float C = fmaf(-lam, L, xo[k]);
-            const float Dv = fminf(fmaxf(C, lb), ub);
-            Ds[r][tx] = Dv;
-            Dn[i * n + j] = Dv;
-            const double dd = (double)Dv - (double)dol[k], cd = (double)C - (double)Dv;
-            s[0] = fma(dd, dd, s[0]);
-            s[1] = fma((double)Dv, (double)Dv, s[1]);
-            s[2] = fma(cd, cd, s[2]);
-            s[3] = fma((double)C, (double)C, s[3]);
+    int tile = blockIdx.x, stage = 0;
+    if (tile < ntiles) tv_stage_load<VEC>(S.st[0], a, P, Q, Dold, (tile / tiles_x) * T, (tile % tiles_x) * T, t);
+    cp_async_commit();
+    for (; tile < ntiles; tile += gridDim.x) {
+        const int next = tile + gridDim.x;
+        if (next < ntiles)
+            tv_stage_load<VEC>(S.st[stage ^ 1], a, P, Q, Dold, (next / tiles_x) * T, (next % tiles_x) * T, t);
+        cp_async_commit();
+        cp_async_wait1();          // this tile's copies have landed (this thread's)
+        __syncthreads();           // ... and every thread's
+        const TvStage &G = S.st[stage];
+        const int i0 = (tile / tiles_x) * T, j0 = (tile % tiles_x) * T;
+        const int j = j0 + tx;
+        // R on rows i0-1 .. i0+T (stage row r), columns j0-1 .. j0+T (stage
+        // column cc + 1): R1 from column j0 + cc, R2 from column j0 - 1 + cc
+        for (int e = t; e < (T + 2) * (T + 2); e += kTvThreads) {
+            const int r = e / (T + 2), cc = e % (T + 2);
+            const float2 p = G.P[r][cc + 1], q = G.Q[r][cc + 1];
+            if (cc >= 1) S.R1s[r][cc - 1] = fmaf(c, p.x - q.x, p.x);
+            if (r >= 1) S.R2s[r - 1][cc] = fmaf(c, p.y - q.y, p.y);
         }
-    }
-    if (hin) {
-        const int r = ty == 0 ? T : tx, cc = ty == 0 ? tx : T;
-        const float L = (R1s[r + 1][cc] - R1s[r][cc]) + (R2s[r][cc + 1] - R2s[r][cc]);
-        Ds[r][cc] = fminf(fmaxf(fmaf(-lam, L, xh), lb), ub);
-    }
-    __syncthreads();
-    // P_new = proj(R + Ltrans(D) / (8 lambda)) on the tile
-    const float inv8l = 1.0f / (8.0f * lam);
+        __syncthreads();
+        // C = Xobs - lambda L(R), D = clamp(C) on the tile (partials) and its halo
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int r = ty + 8 * k, i = i0 + r;
-        if (i < m && j < n) {
-            const float d = Ds[r][tx];
-            float p1 = i < m - 1 ? fmaf(d - Ds[r + 1][tx], inv8l, R1s[r + 1][tx]) : 0.0f;
-            float p2 = j < n - 1 ? fmaf(d - Ds[r][tx + 1], inv8l, R2s[r][tx + 1]) : 0.0f;
-            if (a.iso) {   // P / max(1, |P|): scaled only outside the unit ball
-                const float q2 = fmaf(p1, p1, p2 * p2);
-                if (q2 > 1.0f) {
-                    const float r = rsqrtf(q2);
-                    p1 *= r;
-                    p2 *= r;
-                }
-            } else {
-                p1 = fminf(fmaxf(p1, -1.0f), 1.0f);
-                p2 = fminf(fmaxf(p2, -1.0f), 1.0f);
+        for (int k = 0; k < 4; ++k) {
+            const int r = ty + 8 * k, i = i0 + r;
+            if (i < m && j < n) {
+                const float L = (S.R1s[r + 1][tx] - S.R1s[r][tx]) + (S.R2s[r][tx + 1] - S.R2s[r][tx]);
+                const float C = fmaf(-lam, L, G.X[r][tx]);
+                const float Dv = fminf(fmaxf(C, lb), ub);
+                S.Ds[r][tx] = Dv;
+                Dn[i * n + j] = Dv;
+                const double dd = (double)Dv - (double)G.D[r][tx], cd = (double)C - (double)Dv;
+                s[0] = fma(dd, dd, s[0]);
+                s[1] = fma((double)Dv, (double)Dv, s[1]);
+                s[2] = fma(cd, cd, s[2]);
+                s[3] = fma((double)C, (double)C, s[3]);
             }
-            N[i * n + j] = make_float2(p1, p2);
         }
+        if (ty < 2) {   // the bottom row (warp 0) and the right column (warp 1)
+            const int r = ty == 0 ? T : tx, cc = ty == 0 ? tx : T;
+            if (i0 + r < m && j0 + cc < n) {
+                const float L = (S.R1s[r + 1][cc] - S.R1s[r][cc]) + (S.R2s[r][cc + 1] - S.R2s[r][cc]);
+                S.Ds[r][cc] = fminf(fmaxf(fmaf(-lam, L, G.X[r][cc]), lb), ub);
+            }
+        }
+        __syncthreads();
+        // P_new = proj(R + Ltrans(D) / (8 lambda)) on the tile
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int r = ty + 8 * k, i = i0 + r;
+            if (i < m && j < n) {
+                const float d = S.Ds[r][tx];
+                float p1 = i < m - 1 ? fmaf(d - S.Ds[r + 1][tx], inv8l, S.R1s[r + 1][tx]) : 0.0f;
+                float p2 = j < n - 1 ? fmaf(d - S.Ds[r][tx + 1], inv8l, S.R2s[r][tx + 1]) : 0.0f;
+                if (a.iso) {   // P / max(1, |P|): scaled only outside the unit ball
+                    const float q2 = fmaf(p1, p1, p2 * p2);
+                    if (q2 > 1.0f) {
+                        const float rs = rsqrtf(q2);
+                        p1 *= rs;
+                        p2 *= rs;
+                    }
+                } else {
+                    p1 = fminf(fmaxf(p1, -1.0f), 1.0f);
+                    p2 = fminf(fmaxf(p2, -1.0f), 1.0f);
+                }
+                N[i * n + j] = make_float2(p1, p2);
+            }
+        }
+        __syncthreads();           // the stage and the R / D tiles are free again
+        stage ^= 1;
     }
     double out[4];
     block_sum4(s, out);
-    const unsigned nblocks = gridDim.x * gridDim.y;
+    const unsigned nblocks = gridDim.x;
     if (t == 0) {
-        const size_t b = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
-        for (int k = 0; k < 4; ++k) a.part[4 * b + k] = out[k];
+        for (int k = 0; k < 4; ++k) a.part[4 * (size_t)blockIdx.x + k] = out[k];
         __threadfence();
         last = atomicAdd(&st->arrived, 1u) == nblocks - 1;
     }
@@ -239,7 +314,7 @@ __global__ void __launch_bounds__(kTvThreads, 4) k_tv_iter(const TvArgs a)
     for (unsigned b = t; b < nblocks; b += kTvThreads)
 #pragma unroll
         for (int k = 0; k < 4; ++k) v[k] += __ldcg(a.part + 4 * (size_t)b + k);
-    __shared__ double red[4][kTvThreads];
+    double(*red)[kTvThreads] = reinterpret_cast<double(*)[kTvThreads]>(tv_smem);   // the stages are free now
 #pragma unroll
     for (int k = 0; k < 4; ++k) red[k][t] = v[k];
     __syncthreads();
@@ -342,7 +417,21 @@ int tv_denoise(TvWorkspace &ws, const float *xobs, int m, int n, double lambda, 
     a.eps = eps;
     a.st = (TvState *)ws.state;
     a.part = ws.part;
-    const dim3 grid((n + kTvTile - 1) / kTvTile, (m + kTvTile - 1) / kTvTile), block(32, kTvThreads / 32);
+    const int tiles_x = (n + kTvTile - 1) / kTvTile, ntiles = tiles_x * ((m + kTvTile - 1) / kTvTile);
+    const dim3 block(32, kTvThreads / 32);
+    const size_t smem = sizeof(TvSmem);
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // 16-byte aligned rows for the vector copies
+    const bool vec = n % 4 == 0 && ((uintptr_t)xobs & 15) == 0;
+    auto kern = vec ? k_tv_iter<true> : k_tv_iter<false>;
+    if ((st = cuda_error(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                         "TV shared memory")) ||
+        (st = cuda_error(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTvThreads, smem),
+                         "TV occupancy")))
+        return st;
+    const int grid = std::min(ntiles, sms * std::max(per_sm, 1));   // persistent blocks
     // D = 0 and P = P_prev = 0 (denoise_bound_mod starts from D = 0, whose
     // projected dual is P = 0, R = P)
     if ((st = cuda_error(cudaMemsetAsync(tv_d(ws.buf, px, 0), 0, sizeof(float) * px, s), "TV start")) ||
@@ -352,7 +441,7 @@ int tv_denoise(TvWorkspace &ws, const float *xobs, int m, int n, double lambda, 
     k_tv_start<<<1, 1, 0, s>>>(a.st, max_iter <= 0 ? 1 : 0);
     TvState h{};
     for (int it = 0; it < max_iter; ++it) {
-        k_tv_iter<<<grid, block, 0, s>>>(a);
+        kern<<<grid, block, smem, s>>>(a, tiles_x, ntiles);
         if ((st = cuda_error(cudaGetLastError(), "TV iteration"))) return st;
         if ((it & 7) == 7 && it != max_iter - 1) {
             if ((st = cuda_error(cudaMemcpyAsync(&h, a.st, sizeof h, cudaMemcpyDeviceToHost, s), "TV state")) ||
