@@ -373,7 +373,9 @@ __global__ void __launch_bounds__(kHaarThreads) k_admm_haar(const HaarArgs a)
         Nv[idx] = nv;
     }
     __syncthreads();
-    // inverse transform, coarsest level first
+    // inverse transform, coarsest level first (unrolled: the block sides are
+    // compile-time powers of two)
+#pragma unroll
     for (int lev = L; lev >= 1; --lev) {
         const int Tl = T >> lev, n = Tl * Tl;
         float c00[kItems], c01[kItems], c10[kItems], c11[kItems];
@@ -419,6 +421,7 @@ __global__ void __launch_bounds__(kHaarThreads) k_admm_haar(const HaarArgs a)
     if (a.final_pass) return;
     __syncthreads();
     // forward transform, finest level first
+#pragma unroll
     for (int lev = 1; lev <= L; ++lev) {
         const int Tl = T >> lev, n = Tl * Tl;
         float x00[kItems], x01[kItems], x10[kItems], x11[kItems];
