@@ -38,7 +38,7 @@ class LoopOpts(ctypes.Structure):
                 ("u", ctypes.c_double), ("max_inner", ctypes.c_int), ("admm_tol", ctypes.c_double),
                 ("no_restart", ctypes.c_int), ("no_adaptive_step", ctypes.c_int), ("cumu_tol", ctypes.c_int),
                 ("wvlt_filter_len", ctypes.c_int), ("wvlt_filter", ctypes.c_double * 20),
-                ("wvlt_levels", ctypes.c_int)]
+                ("wvlt_levels", ctypes.c_int), ("mask", ctypes.c_void_p), ("wvlt_mask", ctypes.c_void_p)]
 
 
 class LoopStats(ctypes.Structure):
@@ -146,6 +146,7 @@ def lib():
         "ctprj_wvlt_l1": ([VP, ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, VP, VP], ctypes.c_int),
         "ctprj_wvlt_admm": ([VP, ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                              ctypes.c_double, ctypes.c_int, VP, VP, ctypes.POINTER(ctypes.c_int), VP], ctypes.c_int),
+        "ctprj_wvlt_mask": ([VP, ctypes.c_int, ctypes.c_int, VP, ctypes.c_int, ctypes.c_int, VP, VP], ctypes.c_int),
         "ctprj_error_string": ([ctypes.c_int], ctypes.c_char_p),
         "ctprj_last_error": ([], ctypes.c_char_p),
     }

@@ -150,7 +150,7 @@ class BHCModel:
                     skip_spectrum=False, unfused=False, init_step="fixed", method="npg",
                     thresh=0.0, min_iterations=0, proximal="nonneg", u=0.0, max_inner=100,
                     admm_tol=1e-2, restart=True, adaptive_step=True, cumu_tol=4, wvlt_filter=None,
-                    wvlt_levels=6, stream=None):
+                    wvlt_levels=6, mask=None, wvlt_mask=None, stream=None):
         """The alternating density / spectrum loop, x and Ie updated in place.
         init_step: 'fixed' (first step x_step), 'bb' or 'hessian' (the
         reference's stepSizeInit rules); method: 'npg' (npg/NPG.m) or 'pg'
@@ -164,6 +164,10 @@ class BHCModel:
         opt.adaptiveStep and opt.cumuTol.  proximal 'wvltADMM' (the reference's
         default) regularises with u |Psit(x)|_1 for the wavelet of scaling
         filter wvlt_filter (default daubcqf(2), Haar) and wvlt_levels levels.
+        mask (n x n CUDA tensor, nonzero = reconstructed pixel) is the
+        reference's opt.mask: the density lives on those pixels only;
+        wvlt_mask is maskk, the coefficients of the masked transform (default:
+        those the mask reaches, utils/wvltMask.m).
         Returns a dict with the cost after each iteration, the accepted density
         steps and the device time."""
         import torch
@@ -183,6 +187,14 @@ class BHCModel:
             for j, v in enumerate(wf):
                 opts.wvlt_filter[j] = float(v)
         opts.wvlt_levels = int(wvlt_levels)
+        keep = []
+        for name, m in (("mask", mask), ("wvlt_mask", wvlt_mask)):
+            if m is not None:
+                mb = (m != 0).to(torch.uint8).contiguous()
+                if mb.numel() != pr.img_shape[0] * pr.img_shape[1] or not mb.is_cuda:
+                    raise ValueError("%s: expected an n x n CUDA tensor" % name)
+                keep.append(mb)
+                setattr(opts, name, mb.data_ptr())
         st = LoopStats()
         check(lib().ctprj_bhc_reconstruct(self._m, _dev_ptr(x, pr.img_shape, pr.device),
                                           _dptr(Ie, self.J, torch.float64),

@@ -442,6 +442,15 @@ k_step_terms(const float *__restrict__ x, const float *__restrict__ g, const flo
     }
 }
 
+// x = 0 outside the reconstruction mask (the reference's density is the
+// masked pixel vector, tomography/ConfigCT.m:122-135 with utils/maskFunc.m)
+__global__ void __launch_bounds__(256)
+k_mask_apply(float *__restrict__ x, const unsigned char *__restrict__ mask, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        if (!mask[i]) x[i] = 0.0f;
+}
+
 // Nesterov extrapolation xbar = max(0, x + coef (x - xprev)); per-block
 // partials of sum |xbar - x| (whether the step carries momentum)
 __global__ void __launch_bounds__(256)
@@ -734,13 +743,14 @@ double reduce_fetch(const double *part, int nblocks, double *d_out, cudaStream_t
 // reference's NPG then stops with "a negative step size") is taken by its
 // magnitude.
 int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *d_imea, int mode,
-                         LoopBufs &b, int pgb, double *t_out, cudaStream_t s)
+                         LoopBufs &b, int pgb, double *t_out, cudaStream_t s, const unsigned char *pmask)
 {
     const long long npx = (long long)m->plan->g.n * m->plan->g.n;
     int st = 0;
     if ((st = likelihood(m, d_x, d_Ie, d_imea, b.f, b.sino, s)) ||
         (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.gx, nullptr, s)))
         return st;
+    if (pmask) k_mask_apply<<<pgb, 256, 0, s>>>(b.gx, pmask, npx);
     k_vec_dot<<<pgb, 256, 0, s>>>(b.gx, nullptr, b.gx, npx, b.part);
     const double gg = reduce_fetch(b.part, pgb, b.sum, s, &st);
     if (st) return st;
@@ -761,6 +771,7 @@ int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, con
             (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, b.sino, s)) ||
             (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.xn, nullptr, s)))
             return st;
+        if (pmask) k_mask_apply<<<pgb, 256, 0, s>>>(b.xn, pmask, npx);
         k_vec_dot<<<pgb, 256, 0, s>>>(b.gx, b.xn, b.gx, npx, b.part);
         const double dgd = reduce_fetch(b.part, pgb, b.sum, s, &st) * scale;
         if (st) return st;
@@ -835,6 +846,9 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     TvWorkspace tvw;
     WvltProx wws;
     const int n = m->plan->g.n;
+    const unsigned char *pmask = opts->mask;       // NULL: the whole image
+    const unsigned char *cmask = opts->wvlt_mask;  // NULL: derived from pmask, or all coefficients
+    unsigned char *own_cmask = nullptr;
     int st;
     if ((st = cuda_error(cudaMalloc((void **)&b.gx, sizeof(float) * npx), "loop buffers")) ||
         (st = cuda_error(cudaMalloc((void **)&b.xn, sizeof(float) * npx), "loop buffers")) ||
@@ -871,7 +885,8 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     int max_inner = opts->max_inner > 0 ? opts->max_inner : 100, inner = 0, inner_total = 0, retries = 0;
     auto penalty_of = [&](const float *v, double *out) -> int {   // u TV(v) or u |Psit(v)|_1
         double tvv = 0.0;
-        int e = tv ? tv_value(tvw, v, n, n, iso, b.sum + 3, s) : wvlt_l1(wws, v, n, n, wh, wlh, wlev, b.sum + 3, s);
+        int e = tv ? tv_value(tvw, v, n, n, iso, b.sum + 3, s)
+                   : wvlt_l1(wws, v, n, n, wh, wlh, wlev, b.sum + 3, s, cmask);
         if (!e) e = fetch(&tvv, b.sum + 3, 1, s);
         *out = opts->u * tvv;
         return e;
@@ -896,12 +911,20 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     cudaEventCreate(&es1);
     // alpha = max(alpha, 0) before the NPG / PG object is built (bhc/beamhardenSpline.m:232,236)
     k_npg_extrapolate<<<pgb, 256, 0, s>>>(d_x, d_x, npx, 0.0f, d_x, b.part);
+    if (pmask) k_mask_apply<<<pgb, 256, 0, s>>>(d_x, pmask, npx);
     st = cuda_error(cudaGetLastError(), "loop start");
+    // the wavelet coefficients of the masked transform: given, or those the
+    // mask's pixels reach (utils/wvltMask.m)
+    if (!st && wv && pmask && !cmask) {
+        if (!(st = cuda_error(cudaMalloc((void **)&own_cmask, (size_t)npx), "wavelet mask")) &&
+            !(st = wvlt_mask(wws, pmask, n, n, wh, wlh, wlev, own_cmask, s)))
+            cmask = own_cmask;
+    }
     if (!st)
         st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "loop start");
     cudaEventRecord(e0, s);
     if (!st && opts->init_step != CTPRJ_STEP_FIXED) {
-        st = initial_inverse_step(m, d_x, d_Ie, d_imea, opts->init_step, b, pgb, &t, s);
+        st = initial_inverse_step(m, d_x, d_Ie, d_imea, opts->init_step, b, pgb, &t, s, opts->mask);
         evals += opts->init_step == CTPRJ_STEP_BB ? 2 : 1;
     }
     int done = 0;
@@ -918,8 +941,10 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             double f0 = 0.0, mom = 0.0;
             if ((st = cuda_error(cudaGetLastError(), "extrapolation")) ||
                 (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, b.sino, s)) ||
-                (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.gx, nullptr, s)) ||
-                (st = cuda_error(cudaMemcpyAsync(&mom, b.sum + 1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
+                (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.gx, nullptr, s)))
+                break;
+            if (pmask) k_mask_apply<<<pgb, 256, 0, s>>>(b.gx, pmask, npx);   // the masked gradient
+            if ((st = cuda_error(cudaMemcpyAsync(&mom, b.sum + 1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
                 (st = fetch(&f0, b.f, 1, s)))
                 break;
             ++evals;
@@ -935,12 +960,14 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                 if (reg) {   // xn = proxmapping(xbar - g / t, u / t, admmTol difAlpha, maxInnerItr, x)
                     k_axpy<<<pgb, 256, 0, s>>>(b.xbar, b.gx, (float)(-1.0 / t), npx, b.v);
                     if ((st = cuda_error(cudaGetLastError(), "density step"))) break;
-                    if (tv)   // TV.denoise (utils/TV.m:56-80), which starts from D = 0
+                    if (tv) {   // TV.denoise (utils/TV.m:56-80), which starts from D = 0
                         st = tv_denoise(tvw, b.v, n, n, opts->u / t, 0.0, INFINITY, iso, max_inner,
                                         admm_tol * dif_alpha, b.xn, &inner, s);
-                    else      // admm(Psi, Psit, ., init = x) (npg/admm.m)
+                        if (!st && pmask) k_mask_apply<<<pgb, 256, 0, s>>>(b.xn, pmask, npx);   // mask.a
+                    } else {    // admm(Psi, Psit, ., init = x) (npg/admm.m)
                         st = wvlt_admm(wws, b.v, n, n, wh, wlh, wlev, opts->u / t, admm_tol * dif_alpha, max_inner,
-                                       d_x, b.xn, &inner, s);
+                                       d_x, b.xn, &inner, s, pmask, cmask);
+                    }
                     if (st) break;
                     inner_total += inner;
                     k_step_terms<<<pgb, 256, 0, s>>>(b.xbar, b.gx, b.xn, npx, b.part);
@@ -1077,6 +1104,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     tvw.release(s);
     wws.release(s);
     cudaStreamSynchronize(s);
+    cudaFree(own_cmask);
     b.release();
     return st;
 }

@@ -229,11 +229,17 @@ struct WvltProx {
     void release(cudaStream_t s);
 };
 // alpha = argmin 1/2 |alpha - a|^2 + I(alpha >= 0) + u |W alpha|_1 by npg/admm.m
+// (pmask: pixels of the reconstruction, alpha = 0 elsewhere; cmask: the
+// coefficients of the masked transform, maskk; either NULL for all)
 int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h, int lh, int levels, double u,
-              double rel_tol, int max_itr, const float *init, float *alpha, int *iterations, cudaStream_t s);
-// *d_out = |W x|_1 in FP64 (device)
+              double rel_tol, int max_itr, const float *init, float *alpha, int *iterations, cudaStream_t s,
+              const unsigned char *pmask = nullptr, const unsigned char *cmask = nullptr);
+// *d_out = |W x|_1 in FP64 (device), over the coefficients of cmask (NULL: all)
 int wvlt_l1(WvltProx &ws, const float *x, int rows, int cols, const double *h, int lh, int levels, double *d_out,
-            cudaStream_t s);
+            cudaStream_t s, const unsigned char *cmask = nullptr);
+// cmask = the coefficients that the pixels of pmask reach (utils/wvltMask.m)
+int wvlt_mask(WvltProx &ws, const unsigned char *pmask, int rows, int cols, const double *h, int lh, int levels,
+              unsigned char *cmask, cudaStream_t s);
 
 // launchers (projector.cu)
 // the quad image of the forward pass (projector.cu): (half + 1) rows of

@@ -73,6 +73,7 @@ struct AnaArgs {
     float *s0, *s1, *nu;
     double u;
     double *part;             // per-block partials of this level (2 per block)
+    const unsigned char *cmask;   // coefficient mask (maskk): coefficients outside are zero; NULL: all
 };
 
 struct SynArgs {
@@ -89,6 +90,7 @@ struct SynArgs {
     float *out;               // output block, row stride ldo
     int ldo;
     const float *a;           // ADMM: alpha = max((a + rho x) / (1 + rho), 0), stride ldo
+    const unsigned char *pmask;   // ADMM: pixel mask, alpha = 0 outside; NULL: all pixels
 };
 
 // v mod n in [0, n): a long filter can reach several periods of a small block
@@ -151,10 +153,12 @@ __global__ void __launch_bounds__(kWvThreads) k_wvlt_analysis(const AnaArgs a)
         const int pos[4] = {k * a.ldy + l + Ch, (k + Rh) * a.ldy + l, (k + Rh) * a.ldy + l + Ch, k * a.ldy + l};
         const int nfin = a.last ? 4 : 3;
         if (!a.last) a.ll[(size_t)k * a.ldll + l] = ll;
+        const unsigned char *cm = a.cmask;
         if (a.epi == kEpiStore) {
-            for (int q = 0; q < nfin; ++q) a.y[pos[q]] = v[q];
+            for (int q = 0; q < nfin; ++q) a.y[pos[q]] = (!cm || cm[pos[q]]) ? v[q] : 0.0f;
         } else if (a.epi == kEpiL1) {
-            for (int q = 0; q < nfin; ++q) p0 += fabs((double)v[q]);
+            for (int q = 0; q < nfin; ++q)
+                if (!cm || cm[pos[q]]) p0 += fabs((double)v[q]);
         } else {   // ADMM: s = soft(v - nu, u / rho), nu = nu + s - v
             const AdmmState *st = a.st;
             const int cur = st->iter & 1;
@@ -163,6 +167,11 @@ __global__ void __launch_bounds__(kWvThreads) k_wvlt_analysis(const AnaArgs a)
             const float mul = (float)st->nu_mul, thr = (float)(a.u / st->rho);
             for (int q = 0; q < nfin; ++q) {
                 const int p = pos[q];
+                if (cm && !cm[p]) {   // not a coefficient of the masked transform
+                    a.nu[p] = 0.0f;
+                    snew[p] = 0.0f;
+                    continue;
+                }
                 const float nue = mul * a.nu[p];
                 const float w = v[q] - nue;
                 const float sn = w > thr ? w - thr : (w < -thr ? w + thr : 0.0f);
@@ -231,7 +240,7 @@ __global__ void __launch_bounds__(kWvThreads) k_wvlt_synthesis(const SynArgs a)
         for (int f = 0; f < 2; ++f) {
             const size_t o = (size_t)(2 * k + e) * a.ldo + 2 * l + f;
             float v = x[e][f];
-            if (a.a) v = fmaxf(fmaf(rho, v, a.a[o]) / (1.0f + rho), 0.0f);
+            if (a.a) v = (a.pmask && !a.pmask[o]) ? 0.0f : fmaxf(fmaf(rho, v, a.a[o]) / (1.0f + rho), 0.0f);
             a.out[o] = v;
         }
 }
@@ -326,6 +335,7 @@ struct HaarArgs {
     double u;
     double *part;             // per-tile partials, 2 each
     int final_pass;
+    const unsigned char *pmask, *cmask;   // pixel and coefficient masks, or NULL
 };
 
 // coefficient-array index of tile-layout cell (r, c) of tile (ti, tj)
@@ -412,7 +422,8 @@ __global__ void __launch_bounds__(kHaarThreads) k_admm_haar(const HaarArgs a)
     for (int idx = t; idx < T * T; idx += kHaarThreads) {
         const int r = idx >> L, c = idx & (T - 1);
         const size_t gpix = (size_t)(ti * T + r) * a.cols + tj * T + c;
-        const float v = fmaxf(fmaf(rho, W[r * P + c], a.a[gpix]) / (1.0f + rho), 0.0f);
+        const float v = (a.pmask && !a.pmask[gpix]) ? 0.0f
+                                                    : fmaxf(fmaf(rho, W[r * P + c], a.a[gpix]) / (1.0f + rho), 0.0f);
         if (a.final_pass)
             a.alpha[gpix] = v;
         else
@@ -459,6 +470,11 @@ __global__ void __launch_bounds__(kHaarThreads) k_admm_haar(const HaarArgs a)
     for (int idx = t; idx < T * T; idx += kHaarThreads) {
         const int r = idx >> L, c = idx & (T - 1);
         const int gp = haar_coef_index<L>(r, c, ti, tj, a.rows, a.cols);
+        if (a.cmask && !a.cmask[gp]) {   // not a coefficient of the masked transform
+            a.nu[gp] = 0.0f;
+            Sn[gp] = 0.0f;
+            continue;
+        }
         const float v = W[r * P + c];
         const float nue = mul * Nv[idx];
         const float w = v - nue;
@@ -594,7 +610,7 @@ int analysis_blocks(int rows, int cols, int levels)
 // final coefficients into an epilogue (kEpiAdmm, kEpiL1)
 int run_analysis(const WFilter &f, const float *src, int rows, int cols, int levels, float *scratch, int epi,
                  float *y, const AdmmState *st, float *s0, float *s1, float *nu, double u, double *part,
-                 cudaStream_t s)
+                 cudaStream_t s, const unsigned char *cmask = nullptr)
 {
     const size_t quarter = (size_t)(rows / 2) * (cols / 2);
     const float *in = src;
@@ -619,6 +635,7 @@ int run_analysis(const WFilter &f, const float *src, int rows, int cols, int lev
         a.nu = nu;
         a.u = u;
         a.part = part ? part + 2 * (size_t)pbase : nullptr;
+        a.cmask = cmask;
         const dim3 g = level_grid(R, C);
         k_wvlt_analysis<<<g, dim3(kWvThreadsX, kWvThreadsY), 0, s>>>(a);
         pbase += (int)(g.x * g.y);
@@ -632,7 +649,7 @@ int run_analysis(const WFilter &f, const float *src, int rows, int cols, int lev
 // with the ADMM epilogue when a is given
 int run_synthesis(const WFilter &f, const float *y0, const float *y1, const float *nu, int rows, int cols,
                   int levels, float *scratch, const AdmmState *st, int final_pass, const float *a, float *out,
-                  cudaStream_t s)
+                  cudaStream_t s, const unsigned char *pmask = nullptr)
 {
     const size_t quarter = (size_t)(rows / 2) * (cols / 2);
     const float *ll = nullptr;
@@ -652,6 +669,7 @@ int run_synthesis(const WFilter &f, const float *y0, const float *y1, const floa
         g.ldy = cols;
         g.st = st;
         g.final_pass = final_pass;
+        g.pmask = pmask;
         if (lev == 0) {
             g.out = out;
             g.ldo = cols;
@@ -703,7 +721,8 @@ void WvltProx::release(cudaStream_t s)
 }
 
 int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h, int lh, int levels, double u,
-              double rel_tol, int max_itr, const float *init, float *alpha, int *iterations, cudaStream_t s)
+              double rel_tol, int max_itr, const float *init, float *alpha, int *iterations, cudaStream_t s,
+              const unsigned char *pmask, const unsigned char *cmask)
 {
     WFilter f;
     int st;
@@ -729,7 +748,7 @@ int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h,
     const double tol = fmin(1e-3, rel_tol) * scale;
     // s = Psit(init), nu = 0, rho = 1
     if ((st = run_analysis(f, init ? init : a, rows, cols, levels, scratch, kEpiStore, s0, nullptr, nullptr,
-                           nullptr, nullptr, 0.0, nullptr, s)) ||
+                           nullptr, nullptr, 0.0, nullptr, s, cmask)) ||
         (st = cuda_error(cudaMemsetAsync(nu, 0, sizeof(float) * px, s), "wavelet start")))
         return st;
     k_admm_start<<<1, 1, 0, s>>>(dst, tol, max_itr);
@@ -754,14 +773,16 @@ int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h,
     ha.u = u;
     ha.part = ws.part;
     ha.final_pass = 0;
+    ha.pmask = pmask;
+    ha.cmask = cmask;
     AdmmState h_st{};
     for (int it = 0; it <= max_itr + 1; ++it) {
         if (fused) {
             if ((st = launch_admm_haar(levels, ha, s))) return st;
         } else {
-            if ((st = run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 0, a, alpha, s)) ||
+            if ((st = run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 0, a, alpha, s, pmask)) ||
                 (st = run_analysis(f, alpha, rows, cols, levels, scratch, kEpiAdmm, nullptr, dst, s0, s1, nu, u,
-                                   ws.part, s)))
+                                   ws.part, s, cmask)))
                 return st;
             k_admm_scalars<<<1, 256, 0, s>>>(dst, ws.part, nblocks);
         }
@@ -776,7 +797,7 @@ int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h,
     // alpha = max((a + rho Psi(s + nu)) / (1 + rho), 0) from the last s, nu
     ha.final_pass = 1;
     if ((st = fused ? launch_admm_haar(levels, ha, s)
-                    : run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 1, a, alpha, s)) ||
+                    : run_synthesis(f, s0, s1, nu, rows, cols, levels, scratch, dst, 1, a, alpha, s, pmask)) ||
         (st = cuda_error(cudaMemcpyAsync(&h_st, dst, sizeof h_st, cudaMemcpyDeviceToHost, s), "ADMM state")) ||
         (st = cuda_error(cudaStreamSynchronize(s), "ADMM state")))
         return st;
@@ -786,17 +807,53 @@ int wvlt_admm(WvltProx &ws, const float *a, int rows, int cols, const double *h,
 }
 
 int wvlt_l1(WvltProx &ws, const float *x, int rows, int cols, const double *h, int lh, int levels, double *d_out,
-            cudaStream_t s)
+            cudaStream_t s, const unsigned char *cmask)
 {
     WFilter f;
     int st;
     if ((st = check_args(x, d_out, rows, cols, h, lh, levels, &f))) return st;
     if ((st = ws.alloc(rows, cols, s))) return st;
     if ((st = run_analysis(f, x, rows, cols, levels, ws.buf, kEpiL1, nullptr, nullptr, nullptr, nullptr, nullptr, 0.0,
-                           ws.part, s)))
+                           ws.part, s, cmask)))
         return st;
     k_wvlt_sum<<<1, 256, 0, s>>>(ws.part, analysis_blocks(rows, cols, levels), 2, d_out);
     return cuda_error(cudaGetLastError(), "wavelet l1");
+}
+
+// coefficients that any pixel of the mask reaches (utils/wvltMask.m builds
+// the same set as the union of Wt(e_i) != 0 over the mask's pixels e_i): the
+// forward transform of the mask with the filters' magnitudes, whose sums of
+// non-negative terms are positive exactly there
+__global__ void k_mask_to_float(const unsigned char *__restrict__ m, long long n, float *__restrict__ out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = m[i] ? 1.0f : 0.0f;
+}
+__global__ void k_float_to_mask(const float *__restrict__ v, long long n, unsigned char *__restrict__ out)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = v[i] > 0.0f ? 1 : 0;
+}
+
+int wvlt_mask(WvltProx &ws, const unsigned char *pmask, int rows, int cols, const double *h, int lh, int levels,
+              unsigned char *cmask, cudaStream_t s)
+{
+    WFilter f;
+    int st;
+    if ((st = check_args(pmask, cmask, rows, cols, h, lh, levels, &f))) return st;
+    for (int j = 0; j < lh; ++j) {
+        f.h[j] = fabsf(f.h[j]);
+        f.g[j] = fabsf(f.g[j]);
+    }
+    if ((st = ws.alloc(rows, cols, s))) return st;
+    const size_t px = (size_t)rows * cols;
+    float *scratch = ws.buf, *mimg = ws.buf + px / 2, *coef = mimg + px;
+    k_mask_to_float<<<1024, 256, 0, s>>>(pmask, (long long)px, mimg);
+    if ((st = run_analysis(f, mimg, rows, cols, levels, scratch, kEpiStore, coef, nullptr, nullptr, nullptr, nullptr,
+                           0.0, nullptr, s)))
+        return st;
+    k_float_to_mask<<<1024, 256, 0, s>>>(coef, (long long)px, cmask);
+    return cuda_error(cudaGetLastError(), "wavelet mask");
 }
 
 }  // namespace ctprj
@@ -855,6 +912,16 @@ extern "C" int ctprj_wvlt_admm(const float *d_a, int rows, int cols, const doubl
     cudaStream_t s = (cudaStream_t)stream;
     WvltProx ws;
     int st = wvlt_admm(ws, d_a, rows, cols, h, lh, levels, u, rel_tol, max_itr, d_init, d_alpha, iterations, s);
+    ws.release(s);
+    return st;
+}
+
+extern "C" int ctprj_wvlt_mask(const unsigned char *d_mask, int rows, int cols, const double *h, int lh, int levels,
+                               unsigned char *d_maskk, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    WvltProx ws;
+    int st = wvlt_mask(ws, d_mask, rows, cols, h, lh, levels, d_maskk, s);
     ws.release(s);
     return st;
 }

@@ -109,3 +109,18 @@ def get_psi_psit(daub, L):
     (utils/Utils.m:445-469): Psi = midwt(., daubcqf(daub), L), Psit = mdwt."""
     h = daubcqf(daub)
     return (lambda s: midwt(s, h, L)), (lambda x: mdwt(x, h, L))
+
+
+def wvlt_mask(mask, h, L, stream=None):
+    """maskk = wvltMask(mask, L, daub) (utils/wvltMask.m): the coefficients of
+    the L-level transform of filter h that a pixel of mask reaches, as a
+    uint8 CUDA tensor of the mask's shape."""
+    import torch
+    m = (mask != 0).to(torch.uint8).contiguous()
+    if not m.is_cuda or m.dim() != 2:
+        raise TypeError("expected a 2-D CUDA mask")
+    hh, hp, lh = _filt(h)
+    out = torch.empty_like(m)
+    check(lib().ctprj_wvlt_mask(_vp(m), m.shape[0], m.shape[1], hp, lh, int(L), _vp(out),
+                                _stream_handle(stream, m.device.index)))
+    return out

@@ -72,6 +72,12 @@ typedef struct {
     int wvlt_filter_len;        /* CTPRJ_PROX_WVLT_ADMM: scaling filter length (<= 0: 2, Haar) */
     double wvlt_filter[CTPRJ_WVLT_MAX_FILTER];   /* its taps, daubcqf(daub) (unused when <= 0) */
     int wvlt_levels;            /* dwt_L (<= 0: 6, bhc/doBHC.m:33); n divisible by 2^dwt_L */
+    const unsigned char *mask;  /* opt.mask: device n x n bytes, nonzero = a pixel of the
+                                   reconstruction (the density is 0 elsewhere, its gradient
+                                   and proximal maps are restricted to it); NULL: all pixels */
+    const unsigned char *wvlt_mask;  /* maskk: device n x n bytes over the coefficient array,
+                                   the coefficients of Psit (utils/Utils.m:445-469); NULL:
+                                   those the mask reaches (utils/wvltMask.m), or all */
 } ctprj_bhc_loop_opts;
 
 typedef struct {

@@ -60,6 +60,12 @@ int ctprj_wvlt_admm(const float *d_a, int rows, int cols, const double *h, int l
                     double rel_tol, int max_itr, const float *d_init, float *d_alpha, int *iterations,
                     void *stream);
 
+/* d_maskk = wvltMask(d_mask, levels, daub) (utils/wvltMask.m): 1 at every
+ * coefficient of the rows x cols transform that a pixel with d_mask != 0
+ * reaches, else 0 (uint8 images, row-major like the transforms). */
+int ctprj_wvlt_mask(const unsigned char *d_mask, int rows, int cols, const double *h, int lh, int levels,
+                    unsigned char *d_maskk, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -178,7 +178,7 @@ class _Density:
 def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, newton_steps=2,
                 method="npg", init_step="fixed", noise="poisson", skip_spectrum=False, thresh=0.0,
                 min_iterations=0, proximal="nonneg", u=0.0, max_inner=100, admm_tol=1e-2, restart=True,
-                adaptive_step=True, cumu_tol=4, wvlt_h=None, wvlt_levels=6):
+                adaptive_step=True, cumu_tol=4, wvlt_h=None, wvlt_levels=6, mask=None, wvlt_mask=None):
     """The alternating loop; forward(x) -> sinogram and backward(sino) -> image
     are FP64 projector callables.  Returns (x, Ie, stats) with stats holding
     the cost and accepted density step of every iteration.
@@ -195,13 +195,20 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
     "wvltADMM" (the reference's default) regularises with u |Psit(x)|_1: the
     proximal map is admm(Psi, Psit, xbar - g/t, u/t, admmTol * difAlpha,
     maxInnerItr, false, x) (npg/admm.m, wavelet_oracle.admm) with the wavelet
-    of scaling filter wvlt_h (default daubcqf(2)) and wvlt_levels levels."""
+    of scaling filter wvlt_h (default daubcqf(2)) and wvlt_levels levels.
+    mask is opt.mask: the density is the masked pixel vector (held here as the
+    full image with zeros outside), so gradients are gathered on the mask and
+    TV.denoise scatters, denoises and gathers (utils/TV.m:56-80); wvlt_mask is
+    maskk (default: utils/wvltMask.m of the mask)."""
     dens = _Density(forward, backward, k, Ts, imea, noise)
     x = np.maximum(np.asarray(x, np.float64), 0.0)     # alpha = max(alpha, 0): :232, :236
+    pm = 1.0 if mask is None else (np.asarray(mask) != 0).astype(np.float64).reshape(x.shape)
+    x = x * pm
+    grad_of = lambda xx: (lambda fg: (fg[0], fg[1] * pm))(dens.f(xx, Ie, grad=True))
     Ie = np.asarray(Ie, np.float64).copy()
     t = 1.0 / (x_step if x_step > 0 else 1.0)
     if init_step != "fixed":
-        f0, g = dens.f(x, Ie, grad=True)
+        f0, g = grad_of(x)
         gg = float((g * g).sum())
         if init_step == "hessian":
             y = Ts * forward(g).ravel()
@@ -210,7 +217,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
             xx = float((x * x).sum())
             dn = 1e-3 * math.sqrt(xx) if xx > 0 else 1e-3
             scale = dn / math.sqrt(gg)
-            _, g2 = dens.f(x - scale * g, Ie, grad=True)
+            _, g2 = grad_of(x - scale * g)
             t = abs(float(((g - g2) * g).sum()) * scale) / (scale * scale * gg)
         if math.isnan(t):
             t = 1.0
@@ -224,7 +231,9 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
     shape = x.shape if x.ndim == 2 else (int(round(math.sqrt(x.size))),) * 2
     wh = WV.daubcqf(2) if wvlt_h is None else np.asarray(wvlt_h, np.float64)
     if wv:
-        tlv = lambda v: WV.l1_penalty(v.reshape(shape), wh, wvlt_levels)
+        if wvlt_mask is None and mask is not None:
+            wvlt_mask = WV.wvlt_mask(np.asarray(mask).reshape(shape), wh, wvlt_levels)
+        tlv = lambda v: WV.l1_penalty(v.reshape(shape), wh, wvlt_levels, wvlt_mask)
     else:
         tlv = lambda v: TV.tlv(v.reshape(shape), tvkind) if tv else 0.0
     dif_alpha, pen = 1.0, 0.0
@@ -256,7 +265,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
             coef = 0.0 if pg else (theta - 1.0) / theta1
             xbar = np.maximum(0.0, x + coef * (x - xprev))
             mom = float(np.abs(xbar - x).sum())
-            f0, g = dens.f(xbar, Ie, grad=True)
+            f0, g = grad_of(xbar)
             ppp, good, inc, good_mm = 0, True, False, True
             if adaptive_step and cumu >= cumu_tol:
                 t *= 0.5
@@ -270,8 +279,9 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                                                   admm_tol * dif_alpha)
                     else:
                         xn, inner = WV.admm(v, u / t, wh, wvlt_levels, rel_tol=admm_tol * dif_alpha,
-                                            max_itr=max_inner, init=x.reshape(shape))
-                    xn = xn.reshape(xbar.shape)
+                                            max_itr=max_inner, init=x.reshape(shape),
+                                            mask=None if mask is None else pm.reshape(shape), maskk=wvlt_mask)
+                    xn = xn.reshape(xbar.shape) * pm
                     inner_total += inner
                 else:
                     xn = np.maximum(0.0, xbar - g / t)

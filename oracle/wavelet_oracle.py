@@ -146,13 +146,18 @@ def soft_thresh(x, thresh):
     return np.where(x > t, x - t, np.where(x < -t, x + t, 0.0))
 
 
-def admm(a, u, h, L, rel_tol=1e-6, max_itr=1000, init=None):
+def admm(a, u, h, L, rel_tol=1e-6, max_itr=1000, init=None, mask=None, maskk=None):
     """[alpha, pppp] = admm(Psi, Psit, a, u, relativeTol, maxItr, false, init)
-    (npg/admm.m) with Psi = midwt(., h, L), Psit = mdwt(., h, L).  Returns
-    (alpha, iterations)."""
+    (npg/admm.m) with Psi = midwt(., h, L), Psit = mdwt(., h, L), or with
+    masks the operators of utils/Utils.m:445-469 getPsiPsit:
+    Psi = mask.a(midwt(maskk.b(.))), Psit = maskk.a(mdwt(mask.b(.))), the
+    masked vectors held as full arrays with zeros outside.  Returns (alpha,
+    iterations)."""
     a = np.asarray(a, np.float64)
-    Psi = lambda s: midwt(s, h, L)
-    Psit = lambda x: mdwt(x, h, L)
+    pm = 1.0 if mask is None else (np.asarray(mask) != 0).astype(np.float64)
+    cm = 1.0 if maskk is None else (np.asarray(maskk) != 0).astype(np.float64)
+    Psi = lambda s: midwt(s * cm, h, L) * pm
+    Psit = lambda x: mdwt(x * pm, h, L) * cm
     init = a if init is None else np.asarray(init, np.float64)
     rel_tol = min(1e-3, rel_tol)
     scale = float(np.linalg.norm(a))
@@ -188,9 +193,26 @@ def admm(a, u, h, L, rel_tol=1e-6, max_itr=1000, init=None):
     return alpha, pppp
 
 
-def l1_penalty(x, h, L):
-    """pNorm(Psit(x), 1): the 'wvltADMM' penalty (bhc/beamhardenSpline.m:208)."""
-    return float(np.abs(mdwt(x, h, L)).sum())
+def l1_penalty(x, h, L, maskk=None):
+    """pNorm(Psit(x), 1): the 'wvltADMM' penalty (bhc/beamhardenSpline.m:208),
+    over the coefficients of maskk when given."""
+    y = np.abs(mdwt(x, h, L))
+    if maskk is not None:
+        y = y * (np.asarray(maskk) != 0)
+    return float(y.sum())
+
+
+def wvlt_mask(mask, h, L):
+    """maskk = wvltMask(Mask, dwt_L, daub) (utils/wvltMask.m), as there: the
+    union over the mask's pixels e_i of Wt(e_i) != 0."""
+    mask = np.asarray(mask) != 0
+    maskk = np.zeros(mask.shape, bool)
+    test = np.zeros(mask.shape)
+    for idx in zip(*np.nonzero(mask)):
+        test[idx] = 1.0
+        maskk |= mdwt(test, h, L) != 0
+        test[idx] = 0.0
+    return maskk
 
 
 def admm_objective(alpha, a, u, h, L):

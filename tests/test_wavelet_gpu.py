@@ -232,3 +232,56 @@ def test_wvlt_loop_rejects_indivisible_image():
     dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
     with pytest.raises(CtprjError):   # 96 is not divisible by 2^6
         model.reconstruct(dx, dI, torch.from_numpy(m).cuda(), iterations=2, proximal="wvltADMM", u=1e-2)
+
+
+def disc(n, r):
+    yy, xx = np.mgrid[0:n, 0:n]
+    return (xx - (n - 1) / 2) ** 2 + (yy - (n - 1) / 2) ** 2 < r ** 2
+
+
+@pytest.mark.parametrize("daub,L", [(2, 4), (4, 3)])
+def test_wvlt_mask_matches_utils_wvltmask(daub, L):
+    """ctprj_wvlt_mask against the literal restatement of utils/wvltMask.m
+    (the union over the mask's pixels of the transform's nonzeros)."""
+    m = disc(64, 25)
+    h = W.daubcqf(daub)
+    g = wavelet.wvlt_mask(torch.from_numpy(m).cuda(), h, L).cpu().numpy().astype(bool)
+    assert np.array_equal(g, W.wvlt_mask(m, h, L))
+
+
+@pytest.mark.parametrize("method,proximal,daub", [("npg", "wvltADMM", 2), ("pg", "wvltADMM", 4),
+                                                  ("npg", "tviso", 2)])
+def test_masked_loop_tracks_the_fp64_oracle_loop(method, proximal, daub):
+    """The loop with the reference's reconstruction mask (opt.mask, a disc):
+    the density stays on the mask, gradients and proximal maps are the masked
+    ones (maskk derived as utils/wvltMask.m does), and the GPU loop takes the
+    FP64 loop's steps."""
+    import oracle
+    from oracle import bhc_loop_oracle as LO
+    from imgrecsrc_b200 import bhc
+    g, Ts, x_true, k, I_true, m = setup_problem()
+    mk = disc(g.n, 0.45 * g.n)
+    h = W.daubcqf(daub)
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    dx = torch.full((g.n, g.n), 1.0, device="cuda")
+    dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
+    dm = torch.from_numpy(m).cuda()
+    st = model.reconstruct(dx, dI, dm, iterations=10, x_step=1e-3, method=method, proximal=proximal, u=1e-2,
+                           wvlt_filter=h, wvlt_levels=5, mask=torch.from_numpy(mk).cuda())
+    fw = lambda x: oracle.forward(g, x)
+    bw = lambda y: oracle.backward(g, y.reshape(g.np, g.prjWidth))
+    xo, Io, so = LO.reconstruct(fw, bw, k, Ts, np.ones((g.n, g.n)), np.full(20, 1.0 / 20),
+                                m.astype(np.float64), 10, x_step=1e-3, method=method, proximal=proximal,
+                                u=1e-2, wvlt_h=h, wvlt_levels=5, mask=mk)
+    x = dx.cpu().numpy()
+    c, co = np.array(st["cost"]), np.array(so["cost"])
+    ec = float(np.max(np.abs(c - co) / np.abs(co)))
+    steps_equal = np.allclose(st["x_step"], so["x_step"], rtol=1e-12, atol=0)
+    print("masked loop (%s, %s, daub %d): max cost rel %.2e, x rel %.2e, same steps %s, inner %d / %d" % (
+        method, proximal, daub, ec, rel(x, xo), steps_equal, st["inner_iterations"], so["inner_iterations"]))
+    assert not x[~mk].any()
+    assert steps_equal
+    assert ec < 1e-3
+    assert rel(x, xo) < 1e-3
+    assert abs(st["inner_iterations"] - so["inner_iterations"]) <= 0.15 * so["inner_iterations"]

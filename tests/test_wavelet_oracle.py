@@ -117,3 +117,39 @@ def test_admm_iteration_count_and_zero_input():
     assert it == 8
     z, it0 = W.admm(np.zeros((8, 8)), 0.1, W.daubcqf(2), 3)
     assert it0 == 0 and not z.any()
+
+
+def test_wavelet_mask_is_the_reach_of_the_pixels():
+    """utils/wvltMask.m: the union of Wt(e_i) != 0 over the mask's pixels.  A
+    single pixel reaches one coefficient per quadrant and level with the
+    two-tap filter (3 L + 1), more with longer filters; the full image
+    reaches every coefficient."""
+    h2, h4 = W.daubcqf(2), W.daubcqf(4)
+    one = np.zeros((32, 32), bool)
+    one[13, 6] = True
+    assert W.wvlt_mask(one, h2, 4).sum() == 3 * 4 + 1
+    assert W.wvlt_mask(one, h4, 3).sum() > 3 * 3 + 1
+    assert W.wvlt_mask(np.ones((16, 16), bool), h4, 2).all()
+
+
+def test_masked_admm_keeps_the_masks():
+    """With masks the ADMM's alpha is zero outside the pixel mask and equals
+    the solution of the masked problem (Chambolle-Pock on the masked
+    operators)."""
+    rng = np.random.default_rng(8)
+    yy, xx = np.mgrid[0:16, 0:16]
+    mask = ((xx - 7.5) ** 2 + (yy - 7.5) ** 2 < 6.5 ** 2).astype(float)
+    h = W.daubcqf(2)
+    maskk = W.wvlt_mask(mask, h, 2).astype(float)
+    a = (rng.standard_normal((16, 16)) + 0.5) * mask
+    al, it = W.admm(a, 0.2, h, 2, rel_tol=1e-9, max_itr=5000, mask=mask, maskk=maskk)
+    assert not al[mask == 0].any()
+    x = np.maximum(a, 0.0)
+    xb = x.copy()
+    y = np.zeros_like(a)
+    for _ in range(6000):   # the same problem over the masked operators
+        y = np.clip(y + W.mdwt(xb * mask, h, 2) * maskk, -0.2, 0.2)
+        xn = np.maximum((x - W.midwt(y * maskk, h, 2) * mask + a) / 2.0, 0.0) * mask
+        xb = 2 * xn - x
+        x = xn
+    assert np.linalg.norm(al - x) / np.linalg.norm(x) < 1e-3
