@@ -2,7 +2,6 @@
 (include/ctprj_wavelet.h) against the reference's compiled rwt cores
 (tests/golden/rwt_golden.npz) and the FP64 restatement of npg/admm.m
 (oracle/wavelet_oracle.py)."""
-import ctypes
 import os
 
 import numpy as np
