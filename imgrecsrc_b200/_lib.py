@@ -38,7 +38,8 @@ class LoopOpts(ctypes.Structure):
                 ("u", ctypes.c_double), ("max_inner", ctypes.c_int), ("admm_tol", ctypes.c_double),
                 ("no_restart", ctypes.c_int), ("no_adaptive_step", ctypes.c_int), ("cumu_tol", ctypes.c_int),
                 ("wvlt_filter_len", ctypes.c_int), ("wvlt_filter", ctypes.c_double * 20),
-                ("wvlt_levels", ctypes.c_int), ("mask", ctypes.c_void_p), ("wvlt_mask", ctypes.c_void_p)]
+                ("wvlt_levels", ctypes.c_int), ("mask", ctypes.c_void_p), ("wvlt_mask", ctypes.c_void_p),
+                ("pre_steps", ctypes.c_int)]
 
 
 class LoopStats(ctypes.Structure):

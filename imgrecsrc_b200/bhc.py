@@ -150,7 +150,7 @@ class BHCModel:
                     skip_spectrum=False, unfused=False, init_step="fixed", method="npg",
                     thresh=0.0, min_iterations=0, proximal="nonneg", u=0.0, max_inner=100,
                     admm_tol=1e-2, restart=True, adaptive_step=True, cumu_tol=4, wvlt_filter=None,
-                    wvlt_levels=6, mask=None, wvlt_mask=None, stream=None):
+                    wvlt_levels=6, mask=None, wvlt_mask=None, pre_steps=2, stream=None):
         """The alternating density / spectrum loop, x and Ie updated in place.
         init_step: 'fixed' (first step x_step), 'bb' or 'hessian' (the
         reference's stepSizeInit rules); method: 'npg' (npg/NPG.m) or 'pg'
@@ -167,7 +167,8 @@ class BHCModel:
         mask (n x n CUDA tensor, nonzero = reconstructed pixel) is the
         reference's opt.mask: the density lives on those pixels only;
         wvlt_mask is maskk, the coefficients of the masked transform (default:
-        those the mask reaches, utils/wvltMask.m).
+        those the mask reaches, utils/wvltMask.m).  pre_steps is opt.preSteps
+        (2, the BHC driver's default).
         Returns a dict with the cost after each iteration, the accepted density
         steps and the device time."""
         import torch
@@ -187,6 +188,7 @@ class BHCModel:
             for j, v in enumerate(wf):
                 opts.wvlt_filter[j] = float(v)
         opts.wvlt_levels = int(wvlt_levels)
+        opts.pre_steps = int(pre_steps)
         keep = []
         for name, m in (("mask", mask), ("wvlt_mask", wvlt_mask)):
             if m is not None:

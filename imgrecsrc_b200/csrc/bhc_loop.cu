@@ -786,20 +786,22 @@ int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, con
 }  // namespace
 
 // The density step follows the reference's NPG class (npg/NPG.m main, with
-// the projection on x >= 0 or the TV denoising of tv.cu as the proximal map),
-// or its PG class (npg/PG.m: the same without extrapolation and restart):
+// the projection on x >= 0, the TV denoising of tv.cu or the wavelet ADMM of
+// wavelet.cu as the proximal map), or its PG class (npg/PG.m: the same
+// without extrapolation and restart):
 //   theta' = (1 + sqrt(1 + 4 theta^2)) / 2,  xbar = max(0, x + (theta-1)/theta' (x - xprev));
 //   f, grad at xbar;  candidate xn = max(0, xbar - grad / t), accepted when
 //   f(xn) <= f(xbar) + grad.(xn - xbar) + t/2 |xn - xbar|^2 (utils/Utils.m
 //   majorizationHolds); on failure t /= 0.5 (at most 20 times); in the first
-//   10 iterations a success is retried with t *= 0.5 while it holds (at most
-//   17 times); after 4 consecutive first-try successes t *= 0.5 once (failure
+//   preSteps iterations a success is retried with t *= 0.5 while it holds (at
+//   most 17 times); after 4 consecutive first-try successes t *= 0.5 once (failure
 //   of that try raises the count needed by 4);
 //   if f(xn) exceeds the cost of the previous iteration: restart without
 //   momentum (theta = 1) when xbar != x, else keep x when the majorisation
 //   failed or f(xbar) < f(xn) (PG: keep x when the majorisation failed or the
 //   cost rose).  With a TV map the candidate is TV.denoise(xbar - grad / t,
-//   u / t) to tolerance admmTol * difAlpha, the cost carries u TV, and before
+//   u / t) to tolerance admmTol * difAlpha (with the wavelet map admm(..., x)),
+//   the cost carries u TV (u |Psit x|_1), and before
 //   x is kept the step is retried with admmTol / 10 (down to 1e-6) or
 //   maxInnerItr * 10 (up to 1000); those retries cannot change an exact
 //   projection and are not taken for it.  The reference's reset of t to the
@@ -876,7 +878,9 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
     int p = 0, cumu = 0, cumu_tol = opts->cumu_tol > 0 ? opts->cumu_tol : 4, evals = 0, restarts = 0,
         newton_done = 0, conv = 0, converged = 0;
     const bool adaptive = !opts->no_adaptive_step, restart_on = !opts->no_restart;
-    const int pre_steps = 10;
+    // opt.preSteps, which the BHC driver sets on its NPG / PG object
+    // (bhc/beamhardenSpline.m:74, :304; the classes' own default is 10)
+    const int pre_steps = opts->pre_steps > 0 ? opts->pre_steps : 2;
     const double shrink = 0.5;
     // the iterative proximal maps' state (npg/NPG.m:11,23-24 and Methods.m difAlpha = 1)
     const bool iso = prox == CTPRJ_PROX_TV_ISO;

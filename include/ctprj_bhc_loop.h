@@ -78,6 +78,9 @@ typedef struct {
     const unsigned char *wvlt_mask;  /* maskk: device n x n bytes over the coefficient array,
                                    the coefficients of Psit (utils/Utils.m:445-469); NULL:
                                    those the mask reaches (utils/wvltMask.m), or all */
+    int pre_steps;              /* opt.preSteps: iterations in which a successful step is
+                                   retried with a larger one (<= 0: 2, the BHC driver's
+                                   default, bhc/beamhardenSpline.m:74, :304) */
 } ctprj_bhc_loop_opts;
 
 typedef struct {

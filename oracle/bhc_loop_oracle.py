@@ -178,7 +178,8 @@ class _Density:
 def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, newton_steps=2,
                 method="npg", init_step="fixed", noise="poisson", skip_spectrum=False, thresh=0.0,
                 min_iterations=0, proximal="nonneg", u=0.0, max_inner=100, admm_tol=1e-2, restart=True,
-                adaptive_step=True, cumu_tol=4, wvlt_h=None, wvlt_levels=6, mask=None, wvlt_mask=None):
+                adaptive_step=True, cumu_tol=4, wvlt_h=None, wvlt_levels=6, mask=None, wvlt_mask=None,
+                pre_steps=2):
     """The alternating loop; forward(x) -> sinogram and backward(sino) -> image
     are FP64 projector callables.  Returns (x, Ie, stats) with stats holding
     the cost and accepted density step of every iteration.
@@ -288,7 +289,7 @@ def reconstruct(forward, backward, k, Ts, x, Ie, imea, iterations, x_step=1.0, n
                 dx = xn - xbar
                 nc = dens.f(xn, Ie)
                 if nc - f0 <= float((g * dx).sum()) + 0.5 * t * float((dx * dx).sum()):
-                    if p <= 10 and ppp < 18 and good:
+                    if p <= pre_steps and ppp < 18 and good:
                         t *= 0.5
                         continue
                     break
