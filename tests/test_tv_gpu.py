@@ -270,3 +270,39 @@ def test_tv_loop_options_without_restart_or_step_growth():
     assert abs(st["inner_iterations"] - so["inner_iterations"]) <= 0.15 * so["inner_iterations"]
     assert float(np.max(np.abs(c - co) / np.abs(co))) < 1e-3
     assert rel(dx.cpu().numpy(), xo) < 1e-3
+
+
+def test_tv_map_at_512_matches_the_fp64_fgp():
+    """A 512^2 image (16 x 16 tiles of the pipelined kernel, several tiles per
+    persistent block): 40 fixed iterations against the FP64 FGP."""
+    X = noisy_image(512, 512, seed=11)
+    D, it = gpu_denoise(X, 0.1, kind="iso", max_iter=40, eps=0.0)
+    Do, ito = TVO.tv_denoise(X.astype(np.float64), 0.1, tv="iso", max_iter=40, eps=0.0)
+    e = rel(D, Do)
+    print("FGP 512^2: rel %.2e" % e)
+    assert it == ito == 40
+    assert e < 2e-4
+
+
+def test_tv_loop_with_bb_start_and_l1_tracks_the_oracle():
+    """PG with 'tvl1' and the reference's default initial step rule ('BB')."""
+    from oracle import bhc_loop_oracle as LO
+    g, Ts, x_true, k, I_true, m = setup_problem()
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    dx = torch.full((g.n, g.n), 1.0, device="cuda")
+    dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
+    dm = torch.from_numpy(m).cuda()
+    kw = dict(x_step=1e-3, method="pg", proximal="tvl1", u=1e-2, init_step="bb")
+    st = model.reconstruct(dx, dI, dm, iterations=10, **kw)
+    fw = lambda x: oracle.forward(g, x)
+    bw = lambda y: oracle.backward(g, y.reshape(g.np, g.prjWidth))
+    xo, Io, so = LO.reconstruct(fw, bw, k, Ts, np.ones((g.n, g.n)), np.full(20, 1.0 / 20),
+                                m.astype(np.float64), 10, **kw)
+    c, co = np.array(st["cost"]), np.array(so["cost"])
+    steps_equal = np.allclose(st["x_step"], so["x_step"], rtol=1e-5, atol=0)
+    print("TV loop bb/l1: max cost rel %.2e, x rel %.2e, steps equal %s" % (
+        float(np.max(np.abs(c - co) / np.abs(co))), rel(dx.cpu().numpy(), xo), steps_equal))
+    assert steps_equal
+    assert float(np.max(np.abs(c - co) / np.abs(co))) < 1e-3
+    assert rel(dx.cpu().numpy(), xo) < 1e-3

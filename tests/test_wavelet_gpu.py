@@ -284,3 +284,43 @@ def test_masked_loop_tracks_the_fp64_oracle_loop(method, proximal, daub):
     assert ec < 1e-3
     assert rel(x, xo) < 1e-3
     assert abs(st["inner_iterations"] - so["inner_iterations"]) <= 0.15 * so["inner_iterations"]
+
+
+def test_admm_at_512_matches_the_fp64_restatement():
+    """A 512^2 image, Haar, 6 levels (the fused per-tile iteration over 64
+    tiles): 30 fixed iterations against the FP64 ADMM."""
+    a = phantomish(512, 3) - 0.2
+    h = W.daubcqf(2)
+    al, it = wavelet.admm(dev(a), 0.3, h, 6, relative_tol=0.0, max_itr=29)
+    alo, ito = W.admm(a.astype(np.float32).astype(np.float64), 0.3, h, 6, rel_tol=0.0, max_itr=29)
+    e = rel(al.cpu().numpy(), alo)
+    print("ADMM 512^2: %d / %d iterations, alpha rel %.2e" % (it, ito, e))
+    assert it == ito == 30
+    assert e < 1e-4
+
+
+def test_wvlt_loop_gaussian_noise_tracks_the_oracle():
+    """'wvltADMM' with the Gaussian (log-domain least squares) model."""
+    import oracle
+    from oracle import bhc_loop_oracle as LO
+    from imgrecsrc_b200 import bhc
+    g, Ts, x_true, k, I_true, m = setup_problem()
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    model.set_noise("gaussian")
+    dx = torch.full((g.n, g.n), 1.0, device="cuda")
+    dI = torch.from_numpy(np.full(20, 1.0 / 20)).cuda()
+    dm = torch.from_numpy(m).cuda()
+    kw = dict(x_step=1e-3, method="npg", proximal="wvltADMM", u=1e-3, wvlt_levels=5)
+    st = model.reconstruct(dx, dI, dm, iterations=10, **kw)
+    fw = lambda x: oracle.forward(g, x)
+    bw = lambda y: oracle.backward(g, y.reshape(g.np, g.prjWidth))
+    xo, Io, so = LO.reconstruct(fw, bw, k, Ts, np.ones((g.n, g.n)), np.full(20, 1.0 / 20),
+                                m.astype(np.float64), 10, noise="gaussian", **kw)
+    c, co = np.array(st["cost"]), np.array(so["cost"])
+    steps_equal = np.allclose(st["x_step"], so["x_step"], rtol=1e-12, atol=0)
+    print("wvlt loop gaussian: max cost rel %.2e, x rel %.2e, steps equal %s" % (
+        float(np.max(np.abs(c - co) / np.abs(co))), rel(dx.cpu().numpy(), xo), steps_equal))
+    assert steps_equal
+    assert float(np.max(np.abs(c - co) / np.abs(co))) < 1e-3
+    assert rel(dx.cpu().numpy(), xo) < 1e-3
