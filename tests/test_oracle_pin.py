@@ -3,7 +3,8 @@
 The FP64 and FP32 restatements in oracle/ are compared with fixtures that the
 reference's own prj/cpuPrj.c and prj/parPrj.c produced (tests/golden/, made by
 make_golden.py), and, where the compiled reference is present in oracle/_ref,
-with live runs of it at a BASELINE-sized configuration.
+with live runs of it on the parallel 256^2 / 180-view and fan 512^2 /
+360-view geometries.
 """
 import types
 
@@ -93,7 +94,7 @@ def test_weight_matches_reference_getweight():
         assert abs(oracle.weight(*c) - ref.weight(*c)) < 1e-13
 
 
-def test_fp64_restatement_matches_live_reference_baseline_size():
+def test_fp64_restatement_matches_live_reference_par256_fan512():
     if not ref.available():
         pytest.skip("compiled reference not present")
     rng = np.random.default_rng(7)
