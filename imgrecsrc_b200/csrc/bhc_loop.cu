@@ -18,6 +18,7 @@
 //                 (FP64 Cholesky, diagonal lifted until positive definite as
 //                 bhc/ActiveSet.m:62-76 lifts the eigenvalues), then a line
 //                 search shrinking the step by 0.8 (ActiveSet stepShrnk).
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -29,22 +30,35 @@
 
 namespace ctprj {
 
-constexpr int kIeChunk = 64;          // rays per shared-memory chunk
-constexpr int kIeThreads = 256;
 constexpr int kMaxH = kMaxJ * (kMaxJ + 1) / 2;
 
-// The spectrum model at Ie from the column-major basis matrix A (J x nrays),
-// in two passes whose per-block partials share one layout,
+// The basis matrix A (b_j(s_i), J <= 32 functions x nrays rays) of the
+// spectrum step is stored in blocks of four rays: block c holds the 32 x 4
+// values of rows j < 32 and rays 4c .. 4c + 3, row by row.  A warp's load of
+// one row for 32 consecutive rays then reads eight whole 32-byte sectors, and
+// the tensor-core fragments of four rays x eight rows are one contiguous
+// 256-byte segment.  Rows J .. 31 are never read.
+__host__ __device__ __forceinline__ size_t ie_index(int j, long long i)
+{
+    return ((size_t)(i >> 2) * 32 + j) * 4 + (size_t)(i & 3);
+}
+__host__ __device__ __forceinline__ size_t ie_elems(long long nrays) { return (size_t)((nrays + 3) >> 2) * 128; }
+
+// The spectrum model at Ie from the basis matrix A, in two passes whose
+// per-block partials share one layout,
 // part[block * (1 + J + J(J+1)/2)] = {f, g (J), upper triangle of H}:
 //  k_ie_rays  one thread per ray: Ir = A_i . Ie, the likelihood term into f,
 //             r_i = df/dIr and sqrt(q_i) (q: the model curvature, >= 0 for
 //             both noise models) into per-ray arrays;
-//  k_ie_gh    per chunk of kIeChunk rays the block stages the rows
-//             sqrt(q_i) A_i in shared memory while it accumulates
-//             g_j = sum_i A_ij r_i; H = sum_i (sqrt(q_i) A_i)^T (sqrt(q_i) A_i)
-//             is then a small GEMM in which thread (tj, tk) of a 16 x 16 grid
-//             keeps the 2 x 2 tile of rows 2tj.. and columns 2tk.. in
-//             registers (tiles below the diagonal idle).
+//  k_ie_gh    g = sum_i A_i r_i and H = sum_i q_i A_i A_i^T = W^T W,
+//             W = diag(sqrt q) A^T, on the FP64 tensor cores: a warp takes
+//             four rays at a time, lane (group gr = lane / 4, t = lane % 4)
+//             loading A[j][i] for ray i = 4c + t and rows j = gr, gr + 8,
+//             gr + 16, gr + 24 -- exactly the operand fragments of the MMA
+//             m8n8k4 (an 8 x 4 block of W^T and its 4 x 8 transpose share
+//             them) -- so H accumulates as the 10 upper 8 x 8 tiles of a
+//             32 x 32 matrix by mma.sync (the FP64 kind; tcgen05 has none).
+//             Each warp walks a contiguous range of rays.
 __global__ void __launch_bounds__(256)
 k_ie_rays(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
           const double *__restrict__ Ie, int noise, int stride, double *__restrict__ rr,
@@ -58,7 +72,7 @@ k_ie_rays(const double *__restrict__ A, const float *__restrict__ m, long long n
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
          i += (long long)gridDim.x * blockDim.x) {
         double Ir = 0.0;
-        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + (size_t)j * nrays + i), Is[j], Ir);
+        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + ie_index(j, i)), Is[j], Ir);
         const double mi = (double)m[i];
         const RayTerms t = ray_terms(noise, Ir, mi);
         f += t.f;
@@ -75,66 +89,90 @@ k_ie_rays(const double *__restrict__ A, const float *__restrict__ m, long long n
     }
 }
 
-__global__ void __launch_bounds__(kIeThreads)
+constexpr int kGhWarps = 4;
+
+__device__ __forceinline__ void dmma_acc(double &d0, double &d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(kGhWarps * 32)
 k_ie_gh(const double *__restrict__ A, long long nrays, int J, const double *__restrict__ rr,
         const double *__restrict__ sq, int stride, double *__restrict__ part)
 {
-    // rows read as double2 and kept 16-byte aligned; stride 34 spreads the
-    // column-wise staging writes over the banks
-    __shared__ __align__(16) double Ss[kIeChunk][kMaxJ + 2];
-    __shared__ double gred[8][kIeThreads];
-    const int t = threadIdx.x;
-    const int tj = t >> 4, tk = t & 15;
-    const bool htile = 2 * tj <= 2 * tk + 1 && 2 * tj < J && 2 * tk < J;
-    // staging role: ray rs of the chunk, basis functions js + 4 q (q < 8)
-    const int rs = t % kIeChunk, js = t / kIeChunk;
-    double h00 = 0.0, h01 = 0.0, h10 = 0.0, h11 = 0.0;
-    double g[8];
+    __shared__ double hred[kGhWarps][10][64];
+    __shared__ double gred[kGhWarps][kMaxJ];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gr = lane >> 2, tig = lane & 3;
+    const int nb = (J + 7) >> 3;   // 8-row blocks in use
+    // this warp's contiguous range of four-ray chunks
+    const long long nchunks = (nrays + 3) >> 2;
+    const long long wid = (long long)blockIdx.x * kGhWarps + warp, nw = (long long)gridDim.x * kGhWarps;
+    const long long c0 = nchunks * wid / nw, c1 = nchunks * (wid + 1) / nw;
+    double d[10][2];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) g[q] = 0.0;
-    for (long long c0 = (long long)blockIdx.x * kIeChunk; c0 < nrays; c0 += (long long)gridDim.x * kIeChunk) {
-        const int nc = (int)(nrays - c0 < kIeChunk ? nrays - c0 : kIeChunk);
-        const bool in = rs < nc;
-        const double ri = in ? rr[c0 + rs] : 0.0, si = in ? sq[c0 + rs] : 0.0;
-        __syncthreads();
+    for (int t = 0; t < 10; ++t) d[t][0] = d[t][1] = 0.0;
+    double g[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 2
+    for (long long c = c0; c < c1; ++c) {
+        const long long i = 4 * c + tig;
+        const bool in = i < nrays;
+        const double si = in ? sq[i] : 0.0, ri = in ? rr[i] : 0.0;
+        double w[4];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int j = js + 4 * q;
-            const double a = (in && j < J) ? __ldg(A + (size_t)j * nrays + c0 + rs) : 0.0;
-            g[q] = fma(a, ri, g[q]);
-            Ss[rs][j] = si * a;
+        for (int jb = 0; jb < 4; ++jb) {
+            const int j = jb * 8 + gr;
+            const double a = (in && j < J) ? __ldg(A + ie_index(j, i)) : 0.0;
+            w[jb] = si * a;
+            g[jb] = fma(a, ri, g[jb]);
         }
-        __syncthreads();
-        if (htile) {
-            for (int r = 0; r < nc; ++r) {
-                const double2 a = *reinterpret_cast<const double2 *>(&Ss[r][2 * tj]);
-                const double2 b = *reinterpret_cast<const double2 *>(&Ss[r][2 * tk]);
-                h00 = fma(a.x, b.x, h00);
-                h01 = fma(a.x, b.y, h01);
-                h10 = fma(a.y, b.x, h10);
-                h11 = fma(a.y, b.y, h11);
-            }
-        }
+        int t = 0;
+#pragma unroll
+        for (int jr = 0; jr < 4; ++jr)
+#pragma unroll
+            for (int jc = jr; jc < 4; ++jc, ++t)
+                if (jc < nb) dmma_acc(d[t][0], d[t][1], w[jr], w[jc]);
     }
-    // g: the kIeChunk threads of staging group js hold functions js + 4 q
+    // the block: warp partials through shared memory, summed in a fixed order
+    {
+        int t = 0;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) gred[q][t] = g[q];
+        for (int jr = 0; jr < 4; ++jr)
+#pragma unroll
+            for (int jc = jr; jc < 4; ++jc, ++t) {
+                hred[warp][t][gr * 8 + 2 * tig] = d[t][0];
+                hred[warp][t][gr * 8 + 2 * tig + 1] = d[t][1];
+            }
+    }
+#pragma unroll
+    for (int jb = 0; jb < 4; ++jb) {   // the four lanes of a group hold the same rows
+        g[jb] += __shfl_xor_sync(0xffffffffu, g[jb], 1);
+        g[jb] += __shfl_xor_sync(0xffffffffu, g[jb], 2);
+    }
+    if (tig == 0)
+#pragma unroll
+        for (int jb = 0; jb < 4; ++jb) gred[warp][jb * 8 + gr] = g[jb];
     __syncthreads();
     double *out = part + (size_t)blockIdx.x * stride;
-    if (t < J) {
-        const int grp = t % 4, q = t / 4;
-        double gs = 0.0;
-        for (int u = 0; u < kIeChunk; ++u) gs += gred[q][grp * kIeChunk + u];
-        out[1 + t] = gs;
+    for (int j = threadIdx.x; j < J; j += blockDim.x) {
+        double v = 0.0;
+        for (int ww = 0; ww < kGhWarps; ++ww) v += gred[ww][j];
+        out[1 + j] = v;
     }
-    if (htile) {
-        // entries (j, k), j <= k < J, of this thread's tile into the packed upper triangle
-        const int j0 = 2 * tj, k0 = 2 * tk;
-        double *h = out + 1 + J;
-        h[j0 * J - j0 * (j0 - 1) / 2 + (k0 - j0)] = h00;
-        if (k0 + 1 < J) h[j0 * J - j0 * (j0 - 1) / 2 + (k0 + 1 - j0)] = h01;
-        if (j0 + 1 < J && j0 + 1 <= k0) h[(j0 + 1) * J - (j0 + 1) * j0 / 2 + (k0 - j0 - 1)] = h10;
-        if (k0 + 1 < J) h[(j0 + 1) * J - (j0 + 1) * j0 / 2 + (k0 - j0)] = h11;
+    double *h = out + 1 + J;
+    for (int e = threadIdx.x; e < 10 * 64; e += blockDim.x) {
+        const int t = e >> 6, rc = e & 63;
+        // tile t of the upper 4 x 4 tiles in row order: (0,0) (0,1) (0,2) (0,3) (1,1) ...
+        const int jr = t < 4 ? 0 : t < 7 ? 1 : t < 9 ? 2 : 3;
+        const int jc = jr + t - (jr == 0 ? 0 : jr == 1 ? 4 : jr == 2 ? 7 : 9);
+        const int j = jr * 8 + (rc >> 3), k = jc * 8 + (rc & 7);
+        if (j <= k && k < J) {
+            double v = 0.0;
+            for (int ww = 0; ww < kGhWarps; ++ww) v += hred[ww][t][rc];
+            h[j * J - j * (j - 1) / 2 + (k - j)] = v;
+        }
     }
 }
 
@@ -153,7 +191,7 @@ k_ie_f(const double *__restrict__ A, const float *__restrict__ m, long long nray
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
          i += (long long)gridDim.x * blockDim.x) {
         double Ir = 0.0;
-        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + (size_t)j * nrays + i), Is[j], Ir);
+        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + ie_index(j, i)), Is[j], Ir);
         f += ray_terms(noise, Ir, (double)m[i]).f;
     }
     for (int o = 16; o > 0; o >>= 1) f += __shfl_down_sync(0xffffffffu, f, o);
@@ -171,6 +209,37 @@ __global__ void k_ie_sum(const double *__restrict__ part, int nblocks, int strid
                          double *__restrict__ out)
 {
     sum_partials(part, nblocks, stride, ncols, out);
+}
+
+// the same sums for many columns: block (32 columns x 32 row groups), each
+// thread four interleaved partial sums over its rows, then a fixed tree over
+// the groups -- every column's order is fixed by the launch shape
+__global__ void __launch_bounds__(1024) k_ie_sum_wide(const double *__restrict__ part, int nblocks, int stride,
+                                                      int ncols, double *__restrict__ out)
+{
+    __shared__ double red[32][33];
+    const int cl = threadIdx.x, grp = threadIdx.y, c = blockIdx.x * 32 + cl;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (c < ncols) {
+        auto P = [&](int b) { return part[(size_t)b * stride + c]; };
+        int b = grp;
+        for (; b + 96 < nblocks; b += 128) {
+            a0 += P(b);
+            a1 += P(b + 32);
+            a2 += P(b + 64);
+            a3 += P(b + 96);
+        }
+        if (b < nblocks) a0 += P(b);
+        if (b + 32 < nblocks) a1 += P(b + 32);
+        if (b + 64 < nblocks) a2 += P(b + 64);
+    }
+    red[grp][cl] = (a0 + a1) + (a2 + a3);
+    __syncthreads();
+    for (int h = 16; h > 0; h >>= 1) {
+        if (grp < h) red[grp][cl] += red[grp + h][cl];
+        __syncthreads();
+    }
+    if (grp == 0 && c < ncols) out[c] = red[0][cl];
 }
 
 // Cholesky factorisation, by one warp, of the Jacobi-scaled block
@@ -538,9 +607,9 @@ k_axpy(const float *__restrict__ x, const float *__restrict__ g, float alpha, lo
         out[i] = fmaf(alpha, g[i], x[i]);
 }
 
-// basis matrix from the saved per-ray projections s (already scaled by Ts),
-// column-major: A[j * nrays + i] = b_j(s_i), so that a warp's writes (and every
-// later read) of one basis function are contiguous
+// basis matrix from the saved per-ray projections s (already scaled by Ts):
+// A[ie_index(j, i)] = b_j(s_i), a thread per ray (a warp's writes of one basis
+// function fill whole 32-byte sectors)
 __global__ void __launch_bounds__(256)
 k_basis_from_s(const float *__restrict__ s, long long nrays, const double *__restrict__ tab_g, int J,
                double *__restrict__ A)
@@ -558,7 +627,7 @@ k_basis_from_s(const float *__restrict__ s, long long nrays, const double *__res
             const double eR = exp(-t[2] * si);
             double bj = ((eC - eR) * t[4] - (eL - eC) * t[3]) * is2;
             if (as < t[9]) bj = fma(fma(fma(t[8], si, t[7]), si, t[6]), si, t[5]);
-            A[(size_t)j * nrays + i] = bj;
+            A[ie_index(j, i)] = bj;
             eL = eC;
             eC = eR;
         }
@@ -583,7 +652,7 @@ struct SpectrumWs {
         const int w = 1 + J + J * (J + 1) / 2;
         blocks = nblocks;
         int st;
-        if ((st = cuda_error(cudaMallocAsync((void **)&A, sizeof(double) * nr * J, s), "basis matrix")) ||
+        if ((st = cuda_error(cudaMallocAsync((void **)&A, sizeof(double) * ie_elems(nr), s), "basis matrix")) ||
             (st = cuda_error(cudaMallocAsync((void **)&part, sizeof(double) * nblocks * w, s), "partials")) ||
             (st = cuda_error(cudaMallocAsync((void **)&fgh, sizeof(double) * w, s), "partials")) ||
             (st = cuda_error(cudaMallocAsync((void **)&dir, sizeof(double) * J, s), "partials")) ||
@@ -618,8 +687,7 @@ int sm_count(int dev)
     return sms;
 }
 
-// blocks of the spectrum-model kernels: four per SM (k_ie_gh holds 62
-// registers x 256 threads and 34 KB of shared memory, so four fit)
+// blocks of the spectrum-model kernels: four per SM
 int spectrum_grid(int dev) { return 4 * sm_count(dev); }
 
 template <class T>
@@ -648,8 +716,8 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
     int done = 0;
     for (int it = 0; it < newton_steps && !st; ++it) {
         k_ie_rays<<<ws.blocks, 256, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, m->noise, w, ws.rr, ws.sq, ws.part);
-        k_ie_gh<<<ws.blocks, kIeThreads, 0, s>>>(ws.A, nr, J, ws.rr, ws.sq, w, ws.part);
-        k_ie_sum<<<1, 256, 0, s>>>(ws.part, ws.blocks, w, w, ws.fgh);
+        k_ie_gh<<<ws.blocks, kGhWarps * 32, 0, s>>>(ws.A, nr, J, ws.rr, ws.sq, w, ws.part);
+        k_ie_sum_wide<<<(w + 31) / 32, dim3(32, 32), 0, s>>>(ws.part, ws.blocks, w, w, ws.fgh);
         k_ie_qp<<<1, 32, 0, s>>>(ws.fgh, d_Ie, J, ws.dir, ws.qp_iters);
         if ((st = cuda_error(cudaGetLastError(), "spectrum Newton"))) break;
         if ((st = fetch(&fcur, ws.fgh, 1, s))) break;
