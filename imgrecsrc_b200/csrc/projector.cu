@@ -42,7 +42,7 @@ namespace ctprj {
 #define CTPRJ_FWD_VIEWS 4
 #endif
 #ifndef CTPRJ_FWD_MINBLOCKS
-#define CTPRJ_FWD_MINBLOCKS 6
+#define CTPRJ_FWD_MINBLOCKS 5
 #endif
 #ifndef CTPRJ_BWD_MINBLOCKS
 #define CTPRJ_BWD_MINBLOCKS 4
@@ -242,25 +242,57 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
                 S[1] = fmaf(w, dp, S[1]);
                 S[7] = fmaf(w, dm, S[7]);
             };
-            // two pixels per step, their four gathers issued together (the
-            // second pixel of an odd-length run re-reads x1 and is skipped)
-            for (int x = x0; x <= x1; x += 2) {
-                const bool two = x < x1;
-                const int xb = two ? x + 1 : x;
-                const float jf = (float)(x - x0);
-                const float D0 = fmaf(jf, cRw, r0), D1 = D0 + cRw;
-                const float H0 = FAN ? fmaf(jf, dhbw, hb0) : hb0;
-                const float H1 = FAN ? H0 + dhbw : hb0;
+            // Pixel x0 + j sits at D = fma(j, cRw, r0) (j even) or that of
+            // j - 1 plus cRw (j odd), and likewise for H.  At unit beam width
+            // a ray crosses one to three pixels of a row below 37 degrees of
+            // obliquity and two to four above, so one straight-line step takes
+            // the first three pixels, their gathers issued together and each
+            // predicated on the pixel being in the run (a lane past its run
+            // sends no request), and single steps the rest; per sum the order
+            // of the terms is x0, x0 + 1, ...
+            auto coef = [&](const int j, float &D, float &H) {
+                const float je = (float)(j & ~1);
+                D = fmaf(je, cRw, r0);
+                H = FAN ? fmaf(je, dhbw, hb0) : hb0;
+                if (j & 1) {
+                    D += cRw;
+                    if (FAN) H += dhbw;
+                }
+            };
+            {
+                const bool p1 = x0 < x1, p2 = x0 + 1 < x1;
+                float D0, H0, D1, H1, D2, H2;
+                coef(0, D0, H0);
+                coef(1, D1, H1);
+                coef(2, D2, H2);
                 if (MODE == kModeCount) {
                     nz += (footprint_weight_v(D0, H0, fp) != 0.0f);
-                    if (two) nz += (footprint_weight_v(D1, H1, fp) != 0.0f);
+                    if (p1) nz += (footprint_weight_v(D1, H1, fp) != 0.0f);
+                    if (p2) nz += (footprint_weight_v(D2, H2, fp) != 0.0f);
+                } else {
+                    const float4 pp0 = __ldg(q + x0), pm0 = __ldg(q - x0);
+                    float4 pp1 = {}, pm1 = {}, pp2 = {}, pm2 = {};
+                    if (p1) {
+                        pp1 = __ldg(q + x0 + 1);
+                        pm1 = __ldg(q - x0 - 1);
+                    }
+                    if (p2) {
+                        pp2 = __ldg(q + x0 + 2);
+                        pm2 = __ldg(q - x0 - 2);
+                    }
+                    accumulate(footprint_weight_v(D0, H0, fp), pp0, pm0);
+                    if (p1) accumulate(footprint_weight_v(D1, H1, fp), pp1, pm1);
+                    if (p2) accumulate(footprint_weight_v(D2, H2, fp), pp2, pm2);
+                }
+            }
+            for (int x = x0 + 3; x <= x1; ++x) {
+                float D, H;
+                coef(x - x0, D, H);
+                if (MODE == kModeCount) {
+                    nz += (footprint_weight_v(D, H, fp) != 0.0f);
                     continue;
                 }
-                const float4 pp0 = __ldg(q + x), pm0 = __ldg(q - x);
-                const float4 pp1 = __ldg(q + xb), pm1 = __ldg(q - xb);
-                const float w0 = footprint_weight_v(D0, H0, fp);
-                accumulate(w0, pp0, pm0);
-                if (two) accumulate(footprint_weight_v(D1, H1, fp), pp1, pm1);
+                accumulate(footprint_weight_v(D, H, fp), __ldg(q + x), __ldg(q - x));
             }
         };
         {
@@ -982,8 +1014,10 @@ __global__ void __launch_bounds__(256) k_quad_batch(const BatchArgs a)
     }
 }
 
+// resident blocks asked of the register allocator: as many warps per SM as the
+// per-plan forward
 template <int V>
-__global__ void __launch_bounds__(32 * V, 24 / V) k_forward_batch(const BatchArgs a)
+__global__ void __launch_bounds__(32 * V, 4 * CTPRJ_FWD_MINBLOCKS / V) k_forward_batch(const BatchArgs a)
 {
     __shared__ long long slot;
     for (;;) {
