@@ -72,6 +72,7 @@ k_ie_rays(const double *__restrict__ A, const float *__restrict__ m, long long n
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
          i += (long long)gridDim.x * blockDim.x) {
         double Ir = 0.0;
+#pragma unroll 8
         for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + ie_index(j, i)), Is[j], Ir);
         const double mi = (double)m[i];
         const RayTerms t = ray_terms(noise, Ir, mi);
@@ -191,6 +192,7 @@ k_ie_f(const double *__restrict__ A, const float *__restrict__ m, long long nray
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
          i += (long long)gridDim.x * blockDim.x) {
         double Ir = 0.0;
+#pragma unroll 8
         for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + ie_index(j, i)), Is[j], Ir);
         f += ray_terms(noise, Ir, (double)m[i]).f;
     }
@@ -608,29 +610,49 @@ k_axpy(const float *__restrict__ x, const float *__restrict__ g, float alpha, lo
 }
 
 // basis matrix from the saved per-ray projections s (already scaled by Ts):
-// A[ie_index(j, i)] = b_j(s_i), a thread per ray (a warp's writes of one basis
-// function fill whole 32-byte sectors)
-__global__ void __launch_bounds__(256)
+// A[ie_index(j, i)] = b_j(s_i), a thread per ray.  A block's 128 rays are 32
+// whole four-ray blocks, 32 KB contiguous in A: the values are assembled in
+// shared memory in A's own layout and written out as 16-byte stores, a warp
+// covering 512 contiguous bytes (rows J .. 31 are skipped).
+constexpr int kBasisThreads = 128;
+__global__ void __launch_bounds__(kBasisThreads)
 k_basis_from_s(const float *__restrict__ s, long long nrays, const double *__restrict__ tab_g, int J,
                double *__restrict__ A)
 {
     __shared__ double tab[kMaxJ * kSplStride];
+    __shared__ __align__(16) double stage[kBasisThreads * 32];
     for (int i = threadIdx.x; i < J * kSplStride; i += blockDim.x) tab[i] = tab_g[i];
     __syncthreads();
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
-         i += (long long)gridDim.x * blockDim.x) {
-        const double si = (double)s[i];
-        const double is2 = 1.0 / (si * si), as = fabs(si);
-        double eL = exp(-tab[0] * si), eC = exp(-tab[1] * si);
-        for (int j = 0; j < J; ++j) {
-            const double *t = tab + j * kSplStride;
-            const double eR = exp(-t[2] * si);
-            double bj = ((eC - eR) * t[4] - (eL - eC) * t[3]) * is2;
-            if (as < t[9]) bj = fma(fma(fma(t[8], si, t[7]), si, t[6]), si, t[5]);
-            A[ie_index(j, i)] = bj;
-            eL = eC;
-            eC = eR;
+    const long long nchunks = (nrays + 3) >> 2;
+    for (long long base = (long long)blockIdx.x * kBasisThreads; base < nrays;
+         base += (long long)gridDim.x * kBasisThreads) {
+        const long long i = base + threadIdx.x;
+        double *col = stage + ((threadIdx.x >> 2) * 32) * 4 + (threadIdx.x & 3);   // row j at col[4 j]
+        if (i < nrays) {
+            const double si = (double)s[i];
+            const double is2 = 1.0 / (si * si), as = fabs(si);
+            double eL = exp(-tab[0] * si), eC = exp(-tab[1] * si);
+            for (int j = 0; j < J; ++j) {
+                const double *t = tab + j * kSplStride;
+                const double eR = exp(-t[2] * si);
+                double bj = ((eC - eR) * t[4] - (eL - eC) * t[3]) * is2;
+                if (as < t[9]) bj = fma(fma(fma(t[8], si, t[7]), si, t[6]), si, t[5]);
+                col[4 * j] = bj;
+                eL = eC;
+                eC = eR;
+            }
+        } else {
+            for (int j = 0; j < J; ++j) col[4 * j] = 0.0;
         }
+        __syncthreads();
+        // 16-byte units e = (block, row, half): block e / 64, row (e / 2) % 32
+        const long long c0 = base >> 2;
+        const int nunits = (int)min((long long)kBasisThreads / 4, nchunks - c0) * 64;
+        const double2 *src = reinterpret_cast<const double2 *>(stage);
+        double2 *dst = reinterpret_cast<double2 *>(A + (size_t)c0 * 128);
+        for (int e = threadIdx.x; e < nunits; e += kBasisThreads)
+            if (((e >> 1) & 31) < J) dst[e] = src[e];
+        __syncthreads();
     }
 }
 
@@ -710,7 +732,7 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
     const int J = m->J, w = 1 + J + J * (J + 1) / 2;
     const long long nr = (long long)m->plan->g.np * m->plan->g.W;
     const int dev = m->plan->device;
-    k_basis_from_s<<<4 * sm_count(dev), 256, 0, s>>>(m->d_s, nr, m->d_tab, J, ws.A);
+    k_basis_from_s<<<6 * sm_count(dev), kBasisThreads, 0, s>>>(m->d_s, nr, m->d_tab, J, ws.A);
     int st = cuda_error(cudaGetLastError(), "basis matrix");
     double fcur = 0.0;
     int done = 0;

@@ -72,6 +72,12 @@ CONFIGS = {
     # distant source (the staged backprojection bounds pixel shadows to first
     # order in pixel / source distance), odd size, non-unit pitch
     "fan_far": ct.Geometry(301, 431, 90, 360, 0.9, 1.0, 3000.0),
+    # detector pitch of 2.5 pixels: a ray crosses up to five pixels of a row
+    # (the forward's single steps past the first three) and a pixel's shadow
+    # stays within two or three detectors
+    "par_wide": ct.Geometry(96, 61, 40, 80, 2.5, 1.0, 0.0),
+    # source close to the image: magnification up to 2 at the near edge
+    "fan_wide": ct.Geometry(97, 71, 45, 88, 2.5, 1.0, 150.0),
 }
 
 
