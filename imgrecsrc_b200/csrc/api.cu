@@ -233,7 +233,7 @@ static int build_plan(const ctprj_geometry *geom, int device, ctprj_plan **out)
         return st;
     }
     const char *bk = getenv("CTPRJ_BWD_KERNEL");
-    p->bwd_seg = span < 32 ? 32 : (span < 64 ? 64 : 0);
+    p->bwd_seg = span <= 32 ? 32 : (span <= 64 ? 64 : 0);
     if (bk && strcmp(bk, "direct") == 0) p->bwd_seg = 0;
     *out = p;
     return CTPRJ_OK;
