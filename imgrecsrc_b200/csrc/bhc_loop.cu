@@ -59,35 +59,80 @@ __host__ __device__ __forceinline__ size_t ie_elems(long long nrays) { return (s
 //             them) -- so H accumulates as the 10 upper 8 x 8 tiles of a
 //             32 x 32 matrix by mma.sync (the FP64 kind; tcgen05 has none).
 //             Each warp walks a contiguous range of rays.
-__global__ void __launch_bounds__(256)
-k_ie_rays(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
-          const double *__restrict__ Ie, int noise, int stride, double *__restrict__ rr,
-          double *__restrict__ sq, double *__restrict__ part)
+// One warp walks groups of 16 rays (four blocks of A, 4 KB contiguous): the
+// group arrives in the warp's shared-memory slot by 16-byte cp.async (rows
+// J .. 31 skipped), padded to 132 doubles per block so that the warp's 16
+// (block, ray) columns fall in distinct bank pairs; lanes 2r and 2r + 1 then
+// reduce rows 0..15 and 16..J-1 of ray r and add the halves by one shuffle.
+// per_ray(i, Ir) runs in the even lane of each ray.
+constexpr int kIeWarps = 8;
+constexpr int kIeChunkStride = 132;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
-    __shared__ double Is[kMaxJ];
-    __shared__ double red[8];
-    for (int j = threadIdx.x; j < J; j += blockDim.x) Is[j] = Ie[j];
-    __syncthreads();
-    double f = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
-         i += (long long)gridDim.x * blockDim.x) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <class F>
+__device__ __forceinline__ void ie_walk_rays(const double *__restrict__ A, long long nrays, int J,
+                                             const double *Is, double *wbuf, F &&per_ray)
+{
+    const int lane = threadIdx.x & 31, h = lane & 1, r = lane >> 1;
+    const long long nchunks = (nrays + 3) >> 2, ngroups = (nchunks + 3) >> 2;
+    const long long nw = (long long)gridDim.x * kIeWarps;
+    for (long long gi = (long long)blockIdx.x * kIeWarps + (threadIdx.x >> 5); gi < ngroups; gi += nw) {
+        const long long c0 = gi * 4;
+        const int nunits = (int)min(4LL, nchunks - c0) * 64;   // 16-byte units: block e / 64, row (e % 64) / 2
+        const double *src = A + (size_t)c0 * 128;
+        for (int e = lane; e < nunits; e += 32)
+            if (((e & 63) >> 1) < J) cp_async16(wbuf + (e >> 6) * kIeChunkStride + (e & 63) * 2, src + (size_t)e * 2);
+        cp_async_wait_all();
+        __syncwarp();
+        const double *col = wbuf + (r >> 2) * kIeChunkStride + (r & 3);
+        const int j1 = min(J, 16 * h + 16);
         double Ir = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + ie_index(j, i)), Is[j], Ir);
-        const double mi = (double)m[i];
-        const RayTerms t = ray_terms(noise, Ir, mi);
-        f += t.f;
-        rr[i] = t.r;
-        sq[i] = sqrt(ray_curvature_model(noise, Ir, mi));
+        for (int j = 16 * h; j < j1; ++j) Ir = fma(col[4 * j], Is[j], Ir);
+        Ir += __shfl_xor_sync(0xffffffffu, Ir, 1);
+        const long long i = 4 * c0 + r;
+        if (h == 0 && i < nrays) per_ray(i, Ir);
+        __syncwarp();
     }
+}
+
+__device__ __forceinline__ void ie_block_sum(double f, double *red, double *out)
+{
     for (int o = 16; o > 0; o >>= 1) f += __shfl_down_sync(0xffffffffu, f, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = f;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        part[(size_t)blockIdx.x * stride] = t;
+        *out = t;
     }
+}
+
+__global__ void __launch_bounds__(kIeWarps * 32)
+k_ie_rays(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
+          const double *__restrict__ Ie, int noise, int stride, double *__restrict__ rr,
+          double *__restrict__ sq, double *__restrict__ part)
+{
+    __shared__ double Is[kMaxJ];
+    __shared__ double red[kIeWarps];
+    __shared__ __align__(16) double wb[kIeWarps][4 * kIeChunkStride];
+    for (int j = threadIdx.x; j < J; j += blockDim.x) Is[j] = Ie[j];
+    __syncthreads();
+    double f = 0.0;
+    ie_walk_rays(A, nrays, J, Is, wb[threadIdx.x >> 5], [&](long long i, double Ir) {
+        const double mi = (double)m[i];
+        const RayTerms t = ray_terms(noise, Ir, mi);
+        f += t.f;
+        rr[i] = t.r;
+        sq[i] = sqrt(ray_curvature_model(noise, Ir, mi));
+    });
+    ie_block_sum(f, red, part + (size_t)blockIdx.x * stride);
 }
 
 constexpr int kGhWarps = 4;
@@ -178,32 +223,20 @@ k_ie_gh(const double *__restrict__ A, long long nrays, int J, const double *__re
 }
 
 // per-block partials of f alone (the line search's trial points), written to
-// part[block * stride]: one thread per ray, its basis values read down the
-// columns of A (coalesced across the warp)
-__global__ void __launch_bounds__(256)
+// part[block * stride]
+__global__ void __launch_bounds__(kIeWarps * 32)
 k_ie_f(const double *__restrict__ A, const float *__restrict__ m, long long nrays, int J,
        const double *__restrict__ Ie, int noise, int stride, double *__restrict__ part)
 {
     __shared__ double Is[kMaxJ];
-    __shared__ double red[8];
+    __shared__ double red[kIeWarps];
+    __shared__ __align__(16) double wb[kIeWarps][4 * kIeChunkStride];
     for (int j = threadIdx.x; j < J; j += blockDim.x) Is[j] = Ie[j];
     __syncthreads();
     double f = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nrays;
-         i += (long long)gridDim.x * blockDim.x) {
-        double Ir = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < J; ++j) Ir = fma(__ldg(A + ie_index(j, i)), Is[j], Ir);
-        f += ray_terms(noise, Ir, (double)m[i]).f;
-    }
-    for (int o = 16; o > 0; o >>= 1) f += __shfl_down_sync(0xffffffffu, f, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = f;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        part[(size_t)blockIdx.x * stride] = t;
-    }
+    ie_walk_rays(A, nrays, J, Is, wb[threadIdx.x >> 5],
+                 [&](long long i, double Ir) { f += ray_terms(noise, Ir, (double)m[i]).f; });
+    ie_block_sum(f, red, part + (size_t)blockIdx.x * stride);
 }
 
 // out[c] = sum over blocks of part[b * stride + c] for c < ncols (fixed order, FP64)
@@ -737,7 +770,7 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
     double fcur = 0.0;
     int done = 0;
     for (int it = 0; it < newton_steps && !st; ++it) {
-        k_ie_rays<<<ws.blocks, 256, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, m->noise, w, ws.rr, ws.sq, ws.part);
+        k_ie_rays<<<ws.blocks, kIeWarps * 32, 0, s>>>(ws.A, d_imea, nr, J, d_Ie, m->noise, w, ws.rr, ws.sq, ws.part);
         k_ie_gh<<<ws.blocks, kGhWarps * 32, 0, s>>>(ws.A, nr, J, ws.rr, ws.sq, w, ws.part);
         k_ie_sum_wide<<<(w + 31) / 32, dim3(32, 32), 0, s>>>(ws.part, ws.blocks, w, w, ws.fgh);
         k_ie_qp<<<1, 32, 0, s>>>(ws.fgh, d_Ie, J, ws.dir, ws.qp_iters);
@@ -747,7 +780,7 @@ int spectrum_steps(ctprj_bhc *m, const float *d_imea, double *d_Ie, int newton_s
         bool accepted = false, converged = false;
         for (int ls = 0; ls < 40; ++ls, step *= 0.8) {
             k_ie_trial<<<1, 32, 0, s>>>(d_Ie, ws.dir, ws.fgh, J, step, ws.trial);
-            k_ie_f<<<ws.blocks, 256, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, m->noise, w, ws.part);
+            k_ie_f<<<ws.blocks, kIeWarps * 32, 0, s>>>(ws.A, d_imea, nr, J, ws.trial, m->noise, w, ws.part);
             k_ie_sum<<<1, 256, 0, s>>>(ws.part, ws.blocks, w, 1, ws.f1);
             double fn = 0.0, gd = 0.0;
             if ((st = cuda_error(cudaMemcpyAsync(&fn, ws.f1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
