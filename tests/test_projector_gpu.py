@@ -197,3 +197,31 @@ def test_full_size_fan_properties():
     lhs = (pr.forward(z).double() * y.double()).sum()
     rhs = (xz * Aty).sum()
     assert (abs(lhs - rhs) / (torch.linalg.norm(pr.forward(z).double()) * torch.linalg.norm(y.double()))).item() < 1e-6
+
+
+@pytest.mark.parametrize("d", [0.0, 12000.0])
+def test_4096_adjoint_and_linearity(d):
+    """A 4096^2 image (67 M pixels, a 268 MB quad image, 720 views, 4096
+    bins): the plan's staging capacity and every index at twice the headline
+    size, checked through the adjoint identity and linearity."""
+    g = ct.Geometry(4096, 4096, 720, 720, 1.0, 1.0, d)
+    pr = ct.Projector(g)
+    gen = torch.Generator(device="cuda").manual_seed(21)
+    z = torch.randn(4096, 4096, device="cuda", generator=gen)
+    x = torch.rand(4096, 4096, device="cuda", generator=gen)
+    y = torch.randn(g.np, g.prjWidth, device="cuda", generator=gen)
+    y[:, 0] = 0
+    sz = pr.forward(z).double()
+    s1 = pr.forward(0.5 * x + 2.0 * z).double()
+    s2 = 0.5 * pr.forward(x).double() + 2.0 * sz
+    lin = (torch.linalg.norm(s1 - s2) / torch.linalg.norm(s2)).item()
+    assert lin < 1e-5, lin
+    Aty = pr.backward(y).double()
+    zz = z.double().clone()
+    zz[0, :] = 0
+    zz[:, 0] = 0
+    lhs = (sz * y.double()).sum()
+    rhs = (zz * Aty).sum()
+    err = (abs(lhs - rhs) / (torch.linalg.norm(sz) * torch.linalg.norm(y.double()))).item()
+    assert err < 1e-6, err
+    assert torch.isfinite(Aty).all() and Aty.abs().max().item() > 0
