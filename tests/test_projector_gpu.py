@@ -225,3 +225,19 @@ def test_4096_adjoint_and_linearity(d):
     err = (abs(lhs - rhs) / (torch.linalg.norm(sz) * torch.linalg.norm(y.double()))).item()
     assert err < 1e-6, err
     assert torch.isfinite(Aty).all() and Aty.abs().max().item() > 0
+
+
+def test_full_size_rows_match_the_reference():
+    """Selected views and image rows of the full 2048^2 fan workload against
+    the reference's own cpuPrj.c in FP64 (tests/golden/fullsize_rows.npz,
+    written by make_fullsize_golden.py from the same seeded inputs)."""
+    z = np.load("tests/golden/fullsize_rows.npz")
+    n, W, npv, P, ds, er, d = z["geom"]
+    g = ct.Geometry(int(n), int(W), int(npv), int(P), float(ds), float(er), float(d))
+    pr = ct.Projector(g)
+    x = phantom.ellipse_phantom(g.n, seed=1).astype(np.float32)
+    y = np.random.default_rng(int(z["sino_seed"])).standard_normal((g.np, g.prjWidth)).astype(np.float32)
+    f = host(pr.forward(dev(x)))[z["views"]]
+    b = host(pr.backward(dev(y)))[z["rows"]]
+    ef, eb = rel(f, z["fwd"].astype(np.float64)), rel(b, z["bwd"].astype(np.float64))
+    assert ef < 1e-5 and eb < 1e-5, (ef, eb)
