@@ -134,13 +134,14 @@ def test_invalid_geometry_rejected():
         oracle.forward(geom((32, 45, 16, 18, 1, 1, 0)), np.zeros((32, 32)))
 
 
-def test_fp64_restatement_matches_reference_rows_at_full_size():
-    """The restatement on the full 2048^2 fan workload against the selected
-    rows of the reference's own FP64 output (tests/golden/fullsize_rows.npz)."""
+@pytest.mark.parametrize("case", [0, 1])
+def test_fp64_restatement_matches_reference_rows_at_full_size(case):
+    """The restatement on full-size fan workloads against the selected rows of
+    the reference's own FP64 output (tests/golden/fullsize_rows.npz)."""
     from imgrecsrc_b200 import phantom
     z = np.load("tests/golden/fullsize_rows.npz")
-    g = geom(z["geom"])
+    g = geom(z["c%d_geom" % case])
     x = phantom.ellipse_phantom(g.n, seed=1).astype(np.float32).astype(np.float64)
     y = np.random.default_rng(int(z["sino_seed"])).standard_normal((g.np, g.prjWidth)).astype(np.float32)
-    assert rel(oracle.forward(g, x)[z["views"]], z["fwd"]) < 1e-6
-    assert rel(oracle.backward(g, y.astype(np.float64))[z["rows"]], z["bwd"]) < 1e-6
+    assert rel(oracle.forward(g, x)[z["c%d_views" % case]], z["c%d_fwd" % case]) < 1e-6
+    assert rel(oracle.backward(g, y.astype(np.float64))[z["c%d_rows" % case]], z["c%d_bwd" % case]) < 1e-6

@@ -227,17 +227,21 @@ def test_4096_adjoint_and_linearity(d):
     assert torch.isfinite(Aty).all() and Aty.abs().max().item() > 0
 
 
-def test_full_size_rows_match_the_reference():
-    """Selected views and image rows of the full 2048^2 fan workload against
-    the reference's own cpuPrj.c in FP64 (tests/golden/fullsize_rows.npz,
-    written by make_fullsize_golden.py from the same seeded inputs)."""
+@pytest.mark.parametrize("case", [0, 1])
+def test_full_size_rows_match_the_reference(case):
+    """Selected views and image rows of full-size fan workloads (2048^2 / 1440
+    views; 1024^2 / 720 views) against the reference's own cpuPrj.c in FP64
+    (tests/golden/fullsize_rows.npz, written by make_fullsize_golden.py from
+    the same seeded inputs)."""
     z = np.load("tests/golden/fullsize_rows.npz")
-    n, W, npv, P, ds, er, d = z["geom"]
+    n, W, npv, P, ds, er, d = z["c%d_geom" % case]
     g = ct.Geometry(int(n), int(W), int(npv), int(P), float(ds), float(er), float(d))
     pr = ct.Projector(g)
     x = phantom.ellipse_phantom(g.n, seed=1).astype(np.float32)
     y = np.random.default_rng(int(z["sino_seed"])).standard_normal((g.np, g.prjWidth)).astype(np.float32)
-    f = host(pr.forward(dev(x)))[z["views"]]
-    b = host(pr.backward(dev(y)))[z["rows"]]
-    ef, eb = rel(f, z["fwd"].astype(np.float64)), rel(b, z["bwd"].astype(np.float64))
+    f = host(pr.forward(dev(x)))[z["c%d_views" % case]]
+    b = host(pr.backward(dev(y)))[z["c%d_rows" % case]]
+    ef = rel(f, z["c%d_fwd" % case].astype(np.float64))
+    eb = rel(b, z["c%d_bwd" % case].astype(np.float64))
+    print("case %d: forward rows %.2e, backprojection rows %.2e" % (case, ef, eb))
     assert ef < 1e-5 and eb < 1e-5, (ef, eb)
