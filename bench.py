@@ -11,9 +11,11 @@ the device; forward and backward counts summed).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 runs N independent replicas (the engine is single-GPU; slices shard
-with no collective), launched by torchrun; value = all ranks' updates / the
-slowest rank's time.  --impl reference times the reference's own CPU projector
-(prj/cpuPrj.c compiled unchanged into oracle/_ref) on the host cores.
+with no collective), one process per GPU: without torchrun's environment the
+script starts torchrun itself.  value = all ranks' updates / the slowest rank's
+time.  --impl reference times the reference's own CPU projector (prj/cpuPrj.c
+compiled unchanged into oracle/_ref) on the host cores, on the same workload
+and the same number of steps.
 """
 import argparse
 import ctypes
@@ -32,10 +34,6 @@ METRIC = "fwd+adjoint Gray-px/s & BHC grad-iter/s vs plain path, 1 B200, rel err
 WORKLOAD = dict(workload="fan-beam fwd+backprojection 2048^2, 1440 views/[0,2pi), 2048 bins, "
                          "d=8192 px, float32 ellipse phantom",
                 n=2048, prjWidth=2048, np=1440, prjFull=1440, dSize=1.0, effectiveRate=1.0, d=8192.0)
-# quarter-scale sample of the same geometry for the CPU legs (same views and
-# detector pitch, n = prjWidth = 1024, same magnification)
-CPU_SAMPLE = dict(n=1024, prjWidth=1024, np=1440, prjFull=1440, dSize=1.0, effectiveRate=1.0,
-                  d=4096.0)
 L2_FLUSH_BYTES = 512 << 20   # > 126 MB L2
 # polychromatic (BHC) gradient iteration on the same geometry: two-material
 # phantom (0 / 2.7 / 7.8 g/cm^3), J = 30 b1 coefficients on kappa log-spaced over
@@ -134,18 +132,18 @@ def init_dist():
     return world, rank, local
 
 
-def cpu_reference_run(steps, warmup, threads=None):
+def cpu_reference_run(steps, warmup, w=None):
     """The reference's own prj/cpuPrj.c (oracle/_ref) -- or, where it was not
-    compiled, the oracle's FP32 port -- on the quarter-scale sample: each step
-    is one forward and one backward pass.  Returns (updates/s, seconds, info)."""
+    compiled, the oracle's FP32 port -- on workload w (default: the headline
+    workload itself): each step is one forward and one backward pass over the
+    same phantom as the GPU arm.  Returns (updates/s, median seconds per step,
+    info)."""
     import types
-
-    import numpy as np
 
     import oracle
     from oracle import ref
     from imgrecsrc_b200 import phantom
-    g = types.SimpleNamespace(**CPU_SAMPLE)
+    g = types.SimpleNamespace(**(w or WORKLOAD))
     x = phantom.ellipse_phantom(g.n, seed=1)
     nnz = oracle.forward_nnz(g) + oracle.backward_nnz(g)
     ncores = os.cpu_count() or 1
@@ -169,25 +167,27 @@ def cpu_reference_run(steps, warmup, threads=None):
         step()
         times.append(time.perf_counter() - t0)
     t = statistics.median(times)
-    sample = ("fan %d^2, %d views/[0,2pi), %d bins, d=%g px (quarter-scale of the workload): "
-              "one forward + one backward pass per step, %d timed; %d nonzero updates per step; "
-              "host has %d cores" % (g.n, g.np, g.prjWidth, g.d, steps, nnz, ncores))
+    sample = ("fan %d^2, %d views/[0,2pi), %d bins, d=%g px (the headline workload itself): one "
+              "forward + one backward pass per step, %d timed after %d warm-up; %d nonzero updates "
+              "per step; host has %d cores" % (g.n, g.np, g.prjWidth, g.d, steps, warmup, nnz, ncores))
     return nnz / t / 1e9, t, dict(kind=kind, cores=cores, sample=sample)
 
 
 def reference_arm(args):
+    """The reference's CPU projector on the same workload, metric and step
+    counts as the GPU arm (one full forward + backward pass per step, about
+    6 s each on a 16-core host).  Under torchrun rank 0 alone runs it."""
     world, rank, _ = init_dist()
+    if world != args.gpus:
+        raise SystemExit("bench.py: %d ranks started for --gpus %d" % (world, args.gpus))
     if rank != 0:
         return
-    # bounded: at most 5 timed and 3 warm-up passes of the quarter-scale
-    # sample (about 1.6 s each on a 16-core host)
-    steps = max(1, min(args.steps, 5))
-    warmup = max(0, min(args.warmup, 3))
+    steps, warmup = max(1, args.steps), max(0, args.warmup)
     v, t, info = cpu_reference_run(steps, warmup)
     line = {"metric": METRIC, "value": v, "unit": "Gray-px/s", "n_gpus": args.gpus,
             "steps": steps, "warmup": warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference", "config": dict(WORKLOAD, sample=info["sample"]),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipse phantom)",
+            "impl": "reference", "config": dict(WORKLOAD),
             "cpu_baseline": dict(value=v, unit="Gray-px/s", **info),
             "e2e": {"value": v, "unit": "Gray-px/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -220,6 +220,8 @@ def our_arm(args):
     import torch
 
     world, rank, local = init_dist()
+    if world != args.gpus:
+        raise SystemExit("bench.py: %d ranks started for --gpus %d" % (world, args.gpus))
     torch.cuda.set_device(local)
     pg = None
     if world > 1:
@@ -290,28 +292,31 @@ def our_arm(args):
         kname, kms, kbytes = "k_quad + k_forward<fan>", fwd_ms, 4 * nnz_f + compulsory + 12 * g.n * g.n
     peak, peak_kind = peaks()
     achieved = kbytes / (kms * 1e-3) / 1e9
-    traffic = profiled_traffic().get("k_backward_tiled<fan>" if bwd_ms >= fwd_ms else "k_forward<fan>")
+    prof = profiled_kernels().get("k_backward_tiled<fan>" if bwd_ms >= fwd_ms else "k_forward<fan>", {})
+    traffic = prof.get("dram_bytes_per_launch")
+    issue = issue_roof(prof, kname, kms, clk.get("sm_mhz"), nnz_b if bwd_ms >= fwd_ms else nnz_f)
 
-    # BHC gradient iterations on the polychromatic model's own configuration
-    # (fan 1024^2, 720 views, 1024 bins, J = 20) and on the 2048^2 geometry
-    g3 = ct.Geometry(*geometry_tuple(BHC_WORKLOAD))
-    pr3 = ct.Projector(g3, device=local)
-    bhc_line = {"fan_1024": bhc_leg(ct, g3, pr3, flush, stream, max(3, args.steps // 2), 20,
-                                    "fan 1024^2, 720 views/[0,2pi), 1024 bins, d=2048 px"),
-                "fan_2048": bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2), BHC["J"],
-                                    "fan 2048^2, 1440 views, 2048 bins, d=8192 px")}
-    pr3.close()
-    batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
-    extras_line = extras_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
-    loop_line = None
-    if args.loop_iters > 0:
-        if args.loop_geometry == "1024":
-            gl = ct.Geometry(*geometry_tuple(BHC_WORKLOAD))
-            prl = ct.Projector(gl, device=local)
-            loop_line = loop_leg(ct, gl, prl, args.loop_iters)
-            prl.close()
-        else:
-            loop_line = loop_leg(ct, g, pr, args.loop_iters)
+    bhc_line = batch_line = extras_line = loop_line = None
+    if args.legs == "all":
+        # BHC gradient iterations on the polychromatic model's own configuration
+        # (fan 1024^2, 720 views, 1024 bins, J = 20) and on the 2048^2 geometry
+        g3 = ct.Geometry(*geometry_tuple(BHC_WORKLOAD))
+        pr3 = ct.Projector(g3, device=local)
+        bhc_line = {"fan_1024": bhc_leg(ct, g3, pr3, flush, stream, max(3, args.steps // 2), 20,
+                                        "fan 1024^2, 720 views/[0,2pi), 1024 bins, d=2048 px"),
+                    "fan_2048": bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2), BHC["J"],
+                                        "fan 2048^2, 1440 views, 2048 bins, d=8192 px")}
+        pr3.close()
+        batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
+        extras_line = extras_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
+        if args.loop_iters > 0:
+            if args.loop_geometry == "1024":
+                gl = ct.Geometry(*geometry_tuple(BHC_WORKLOAD))
+                prl = ct.Projector(gl, device=local)
+                loop_line = loop_leg(ct, gl, prl, args.loop_iters)
+                prl.close()
+            else:
+                loop_line = loop_leg(ct, g, pr, args.loop_iters)
 
     # end to end through the reference-facing C ABI: setup() once, then per
     # step gpuPrj(FWD) and gpuPrj(BWD) on pinned host buffers (every call
@@ -355,24 +360,61 @@ def our_arm(args):
                 "ms_per_step": e2e_t * 1e3},
         "gpu_launches": 3 * args.steps,
         "clocks": clk,
-        "bhc": bhc_line,
-        "batch": batch_line,
-        "bhc_loop": loop_line,
-        "extras": extras_line,
     }
+    line["roofline"]["issue"] = issue
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, t, info = cpu_reference_run(1, 0)
+        # the reference's cpuPrj.c on the headline workload itself: 1 warm-up
+        # and 3 timed passes (about 25 s on a 16-core host)
+        v, t, info = cpu_reference_run(3, 1)
         line["cpu_baseline"] = dict(value=v, unit="Gray-px/s", **info)
         par = cpu_parprj_run()
         if par:
             line["cpu_baseline"]["parprj"] = {"kind": "reference", "forward_ms": par[0] * 1e3,
                                               "backward_ms": par[1] * 1e3,
                                               "threads": 32}   # parPrj.c runs 32 pthreads
+    # the secondary legs in full, then (last, so that a tail of the output
+    # keeps it) a compact summary of every leg's headline figures
+    line.update({k: v for k, v in (("bhc", bhc_line), ("batch", batch_line), ("bhc_loop", loop_line),
+                                   ("extras", extras_line)) if v is not None})
+    line["summary"] = summary(line)
     if pg:
         pg.barrier()
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def summary(line):
+    """Headline figures of every leg in one short object (rounded)."""
+    def r(v, k=4):
+        return None if v is None else float("%.*g" % (k, v))
+    c = line["config"]
+    out = {"fwd_ms": r(c["fwd_ms"]), "bwd_ms": r(c["bwd_ms"]), "gray_px_s": r(line["value"]),
+           "e2e_gray_px_s": r(line["e2e"]["value"]),
+           "issue_frac": r((line["roofline"].get("issue") or {}).get("frac"), 3)}
+    if "cpu_baseline" in line:
+        out["cpu_gray_px_s"] = r(line["cpu_baseline"]["value"])
+    for key, b in (line.get("bhc") or {}).items():
+        out["bhc_" + key] = {"fused_grad_iter_per_s": r(b["fused_grad_iter_per_s"]),
+                             "plain_grad_iter_per_s": r(b["plain_grad_iter_per_s"]),
+                             "speedup_vs_plain": r(b["speedup_vs_plain"], 3),
+                             "speedup_vs_plain_min": r(b["speedup_vs_plain_min"], 3)}
+    bt = line.get("batch")
+    if bt:
+        out["batch"] = {"batched_ms": r(bt["batched_ms"]), "per_slice_ms": r(bt["per_slice_ms"]),
+                        "speedup": r(bt["speedup"], 3)}
+    lp = line.get("bhc_loop")
+    if lp:
+        out["loop"] = {k: r(lp[k]["iter_per_s"]) for k in lp if isinstance(lp[k], dict) and "iter_per_s" in lp[k]}
+        out["loop"]["pg_speedup_fused_vs_unfused"] = r(lp["pg_speedup_fused_vs_unfused"], 3)
+        out["loop"]["pg_final_cost"] = r(lp["pg_fused"]["final_cost"], 9)
+    ex = line.get("extras")
+    if ex:
+        out["extras"] = {"fbp_ms": r(ex["fbp_ms"]), "tv_us_per_it": r(ex["tv_denoise"]["us_per_iteration"]),
+                         "wvlt_us_per_it": r(ex["wvlt_admm"]["us_per_iteration"]),
+                         "parprj_fwd_ms": r(ex["parprj"]["forward_ms"]),
+                         "parprj_bwd_ms": r(ex["parprj"]["backward_ms"])}
+    return out
 
 
 def bhc_leg(ct, g, pr, flush, stream, steps, J, workload):
@@ -666,17 +708,89 @@ def extras_leg(ct, g, pr, flush, stream, steps):
     return out
 
 
-# dram__bytes_read.sum + dram__bytes_write.sum per launch from the ncu
-# captures summarised in profiles/ (None until captured)
-def profiled_traffic():
-    """DRAM bytes per launch of each profiled kernel from the committed ncu
-    summary (profiles/traffic.json), or {} when it is absent."""
-    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.json")
+# Per-launch counters of the projection kernels from the committed ncu summary
+# (profiles/projector_counters.json): dram__bytes_read.sum +
+# dram__bytes_write.sum and smsp__inst_executed.sum per launch.
+def profiled_kernels():
+    """Counters per launch of each profiled kernel, or {} when the summary is
+    absent."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "projector_counters.json")
     try:
         with open(path) as f:
-            return {k: v["dram_bytes_per_launch"] for k, v in json.load(f)["kernels"].items()}
+            return json.load(f)["kernels"]
     except (OSError, KeyError, ValueError):
         return {}
+
+
+SMS, SCHEDULERS = 148, 4
+
+
+def issue_roof(prof, kname, kms, sm_mhz, updates):
+    """The roof that binds the projection kernels: warp-instruction issue.  The
+    kernel's warp instructions per launch (ncu smsp__inst_executed.sum) over the
+    issue slots of its CUDA-event duration at the sampled SM clock
+    (148 SMs x 4 schedulers x 1 instruction per cycle)."""
+    inst = prof.get("warp_inst_per_launch")
+    if not inst or not sm_mhz:
+        return None
+    slots = kms * 1e-3 * SMS * SCHEDULERS * sm_mhz * 1e6
+    return {"kernel": kname, "warp_inst_per_launch": inst, "issue_slots_per_launch": slots,
+            "frac": inst / slots, "sm_mhz": sm_mhz,
+            "thread_inst_per_update": 32.0 * inst / updates,
+            "source": "profiles/projector_counters.json (ncu smsp__inst_executed.sum)"}
+
+
+def relaunch(args, argv):
+    """--gpus N > 1 without torchrun's environment: start N ranks of this
+    script under torch.distributed.run on this node (rendezvous on
+    127.0.0.1) and return their exit status."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node=%d" % args.gpus, "--master-addr=127.0.0.1",
+           "--master-port=%d" % port, os.path.abspath(__file__)] + argv
+    return subprocess.run(cmd).returncode
+
+
+def selftest_arm(args):
+    """The multi-rank plumbing without a GPU (gloo): each rank times a small
+    host computation in place of the projection step, and rank 0 prints the
+    bench line with the same world check, MAX-over-ranks time and replica
+    aggregation as the GPU arm."""
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+
+    world, rank, _ = init_dist()
+    if world != args.gpus:
+        raise SystemExit("bench.py: %d ranks started for --gpus %d" % (world, args.gpus))
+    pg = None
+    if world > 1:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        pg = dist
+    a = np.random.default_rng(rank).random((256, 256), dtype=np.float32)
+    for _ in range(max(3, args.warmup)):
+        a @ a
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        a @ a
+    t_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    t_max = max_over_ranks(t_ms, pg, "cpu")
+    updates = 2 * 256 ** 3
+    line = {"metric": "selftest host matmul (not a projector measurement)",
+            "value": replica_value(world, updates, t_max), "unit": "Gflop/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t_max,
+            "rank_ms": t_ms}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def main():
@@ -691,8 +805,17 @@ def main():
     ap.add_argument("--loop-geometry", default="2048", choices=["2048", "1024"],
                     help="reconstruction leg on the 2048^2 workload (config 5) or on the "
                          "1024^2 configuration of the polychromatic model (smaller, for profiling)")
+    ap.add_argument("--legs", default="all", choices=["all", "projector"],
+                    help="projector: the headline step and its end-to-end run only (for profiling)")
+    ap.add_argument("--selftest", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.gpus < 1:
+        ap.error("--gpus must be >= 1")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args, sys.argv[1:]))
+    if args.selftest:
+        selftest_arm(args)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         our_arm(args)

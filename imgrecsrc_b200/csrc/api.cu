@@ -34,7 +34,7 @@ int cuda_error(cudaError_t e, const char *what)
 
 // View angle of view i exactly as the reference forms it (prj/cpuPrj.c:342):
 // ((float)(2 i) * pi_f) / (float)prjFull in float arithmetic.
-static double view_angle(int i, int P)
+double view_angle(int i, int P)
 {
     volatile float th = (float)(2 * i) * kRefPiF;
     th = th / (float)P;
@@ -44,7 +44,7 @@ static double view_angle(int i, int P)
 // View of symmetric image j for base view b: (q_j P/4 + s_j b) mod P, with
 // (q, s) = (0,+)(1,+)(2,+)(3,+)(2,-)(3,-)(4,-)(1,-) (prj/cpuPrj.c:403-460,
 // :117-157).
-static int view_of(int j, int b, int P)
+int view_of(int j, int b, int P)
 {
     static const int q[8] = {0, 1, 2, 3, 2, 3, 4, 1};
     static const int sg[8] = {1, 1, 1, 1, -1, -1, -1, -1};
@@ -52,7 +52,7 @@ static int view_of(int j, int b, int P)
     return v < 0 ? v + P : v;
 }
 
-static int validate(const ctprj_geometry *g)
+int validate_geometry(const ctprj_geometry *g)
 {
     if (!g) return set_error(CTPRJ_EINVAL, "geometry is NULL");
     if (g->n < 1 || g->prjWidth < 1 || g->np < 1)
@@ -76,7 +76,7 @@ static int validate(const ctprj_geometry *g)
     return CTPRJ_OK;
 }
 
-static Geo make_geo(const ctprj_geometry &gm)
+Geo make_geo(const ctprj_geometry &gm)
 {
     Geo g;
     g.n = gm.n;
@@ -95,6 +95,50 @@ static Geo make_geo(const ctprj_geometry &gm)
     g.invEr = 1.0f / gm.effectiveRate;
     g.effRate = gm.effectiveRate;
     return g;
+}
+
+// forward ray set (prj/cpuPrj.c:326-332, :469-475, :632-644): base views
+// b <= prjFull/8, the first ray and the rays per base view
+void fwd_ray_set(const Geo &g, int *nb, int *k0, int *nk)
+{
+    *nb = g.np < g.P / 8 + 1 ? g.np : g.P / 8 + 1;
+    *k0 = (g.W % 2 == 0) ? 1 : 0;
+    *nk = g.fan ? (g.W % 2 == 0 ? g.W - 1 : g.W) : (g.W % 2 == 0 ? g.W / 2 : (g.W + 1) / 2);
+}
+
+void fill_fwd_views(const Geo &g, int nb, FwdView *fv)
+{
+    for (int b = 0; b < nb; ++b) {
+        const double th = view_angle(b, g.P);
+        fv[b].c = cos(th);
+        fv[b].s = sin(th);
+        const bool mirror = b > 0 && (float)b < (float)g.P * 0.125f;
+        for (int j = 0; j < 8; ++j) {
+            const int v = view_of(j, b, g.P);
+            fv[b].out[j] = ((j < 4 || mirror) && v < g.np) ? v : -1;
+        }
+    }
+}
+
+void fill_det_table(const Geo &g, DetEntry *de)
+{
+    for (int k = 0; k < g.W; ++k) {
+        DetEntry &e = de[k];
+        e.t = (double)(k - g.pC) * g.dSize;
+        if (g.fan) {
+            const double bq = sqrt(g.d * g.d + e.t * e.t);
+            e.cB = g.d / bq;
+            e.sB = e.t / bq;
+            e.invbq = (float)(1.0 / bq);
+        } else {
+            e.cB = 1.0;
+            e.sB = 0.0;
+            e.invbq = 0.0f;
+        }
+        e.cBf = (float)e.cB;
+        e.sBf = (float)e.sB;
+        e.pad = 0;
+    }
 }
 
 template <class T>
@@ -144,7 +188,7 @@ struct DeviceGuard {
 
 static int build_plan(const ctprj_geometry *geom, int device, ctprj_plan **out)
 {
-    int st = validate(geom);
+    int st = validate_geometry(geom);
     if (st) return st;
     ctprj_plan *p = new (std::nothrow) ctprj_plan();
     if (!p) return set_error(CTPRJ_ENOMEM, "host allocation failed");
@@ -156,23 +200,11 @@ static int build_plan(const ctprj_geometry *geom, int device, ctprj_plan **out)
     const Geo &g = p->g;
     const int W = g.W, P = g.P, np = g.np;
 
-    // forward ray set (prj/cpuPrj.c:326-332, :469-475, :632-644)
-    p->nb = np < P / 8 + 1 ? np : P / 8 + 1;
-    p->k0 = (W % 2 == 0) ? 1 : 0;
-    p->nk = g.fan ? (W % 2 == 0 ? W - 1 : W) : (W % 2 == 0 ? W / 2 : (W + 1) / 2);
+    fwd_ray_set(g, &p->nb, &p->k0, &p->nk);
     p->nv = g.fan ? P : P / 2;
 
     std::vector<FwdView> fv(p->nb);
-    for (int b = 0; b < p->nb; ++b) {
-        const double th = view_angle(b, P);
-        fv[b].c = cos(th);
-        fv[b].s = sin(th);
-        const bool mirror = b > 0 && (float)b < (float)P * 0.125f;
-        for (int j = 0; j < 8; ++j) {
-            const int v = view_of(j, b, P);
-            fv[b].out[j] = ((j < 4 || mirror) && v < np) ? v : -1;
-        }
-    }
+    fill_fwd_views(g, p->nb, fv.data());
     std::vector<BwdView> bv(p->nv);
     for (int i = 0; i < p->nv; ++i) {
         BwdView &e = bv[i];
@@ -195,23 +227,7 @@ static int build_plan(const ctprj_geometry *geom, int device, ctprj_plan **out)
         }
     }
     std::vector<DetEntry> de(W);
-    for (int k = 0; k < W; ++k) {
-        DetEntry &e = de[k];
-        e.t = (double)(k - g.pC) * g.dSize;
-        if (g.fan) {
-            const double bq = sqrt(g.d * g.d + e.t * e.t);
-            e.cB = g.d / bq;
-            e.sB = e.t / bq;
-            e.invbq = (float)(1.0 / bq);
-        } else {
-            e.cB = 1.0;
-            e.sB = 0.0;
-            e.invbq = 0.0f;
-        }
-        e.cBf = (float)e.cB;
-        e.sBf = (float)e.sB;
-        e.pad = 0;
-    }
+    fill_det_table(g, de.data());
 
     DeviceGuard dg(device);
     if ((st = dg.status)) { delete p; return st; }

@@ -202,6 +202,16 @@ struct PlanDevice {
 int set_error(int status, const char *fmt, ...);
 int cuda_error(cudaError_t e, const char *what);
 
+// geometry and host-side tables of a plan (api.cu), shared by every entry
+// point that builds them (plans and the allocation-free forward)
+int validate_geometry(const ctprj_geometry *g);
+Geo make_geo(const ctprj_geometry &gm);
+double view_angle(int i, int P);
+int view_of(int j, int b, int P);
+void fwd_ray_set(const Geo &g, int *nb, int *k0, int *nk);
+void fill_fwd_views(const Geo &g, int nb, FwdView *fv);   // fv[nb]
+void fill_det_table(const Geo &g, DetEntry *de);          // de[prjWidth]
+
 // buffers of the TV proximal map (tv.cu): D, P1, P2 double-buffered, R1, R2
 // (8 images), per-block FP64 partials and the device-side iteration state
 struct TvWorkspace {

@@ -25,8 +25,12 @@
 //
 // The first call on each device looks up the device addresses of the arrays
 // (cudaGetSymbolAddress, with that device current); make that first call
-// before any stream capture.
-#include <cmath>
+// before any stream capture.  The addresses are kept for the life of the
+// process: a caller that tears the device's context down (cudaDeviceReset)
+// and then calls again would hand the kernels stale addresses, so callers of
+// this entry point must not reset the device.  A call on a stream that is
+// being captured returns CTPRJ_EINVAL: its table uploads read static host
+// buffers that every later call overwrites.
 #include <cstring>
 #include <mutex>
 
@@ -83,22 +87,6 @@ static int noalloc_symbols(int dev, NoAllocSymbols *out)
     return CTPRJ_OK;
 }
 
-// the reference's float-formed view angle (prj/cpuPrj.c:342)
-static double noalloc_view_angle(int i, int P)
-{
-    volatile float th = (float)(2 * i) * kRefPiF;
-    th = th / (float)P;
-    return (double)th;
-}
-
-static int noalloc_view_of(int j, int b, int P)
-{
-    static const int q[8] = {0, 1, 2, 3, 2, 3, 4, 1};
-    static const int sg[8] = {1, 1, 1, 1, -1, -1, -1, -1};
-    int v = (q[j] * (P / 4) + sg[j] * b) % P;
-    return v < 0 ? v + P : v;
-}
-
 }  // namespace ctprj
 
 using namespace ctprj;
@@ -106,79 +94,41 @@ using namespace ctprj;
 extern "C" int ctprj_forward_noalloc(const ctprj_geometry *geom, const float *d_img,
                                      float *d_sino, void *stream)
 {
-    if (!geom || !d_img || !d_sino) return set_error(CTPRJ_EINVAL, "NULL geometry or buffer");
+    if (!d_img || !d_sino) return set_error(CTPRJ_EINVAL, "NULL image or sinogram");
+    int st = validate_geometry(geom);
+    if (st) return st;
     const ctprj_geometry &gm = *geom;
-    if (gm.n < 1 || gm.prjWidth < 1 || gm.np < 1 || gm.prjFull < 4 || gm.prjFull % 4 != 0 ||
-        gm.np > gm.prjFull || !(gm.dSize > 0.0f) || !(gm.effectiveRate > 0.0f) ||
-        !std::isfinite(gm.dSize) || !std::isfinite(gm.effectiveRate) || !std::isfinite(gm.d))
-        return set_error(CTPRJ_EINVAL, "invalid geometry (n=%d prjWidth=%d np=%d prjFull=%d)", gm.n,
-                         gm.prjWidth, gm.np, gm.prjFull);
     if (gm.n > kNoAllocMaxN || gm.prjWidth > kNoAllocMaxW || gm.prjFull > kNoAllocMaxP)
         return set_error(CTPRJ_ERANGE,
                          "ctprj_forward_noalloc is limited to n <= %d, prjWidth <= %d and "
                          "prjFull <= %d (got n=%d prjWidth=%d prjFull=%d); use the plan API",
                          kNoAllocMaxN, kNoAllocMaxW, kNoAllocMaxP, gm.n, gm.prjWidth, gm.prjFull);
+    cudaStream_t s = (cudaStream_t)stream;
+    // The table uploads below read the static host tables, which the next call
+    // overwrites: a captured upload would replay whatever a later call left
+    // there, so a call on a capturing stream is refused.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if ((st = cuda_error(cudaStreamIsCapturing(s, &cap), "cudaStreamIsCapturing"))) return st;
+    if (cap != cudaStreamCaptureStatusNone)
+        return set_error(CTPRJ_EINVAL, "ctprj_forward_noalloc was called on a stream that is being captured");
 
     // a plan on the stack whose tables and scratch are the static arrays
     ctprj_plan p;
     memset(&p, 0, sizeof p);
     p.geom = gm;
-    Geo &g = p.g;
-    g.n = gm.n;
-    g.W = gm.prjWidth;
-    g.np = gm.np;
-    g.P = gm.prjFull;
-    g.pC = gm.prjWidth / 2;
-    g.half = (gm.n - 1) / 2;
-    g.h2 = gm.n / 2;
-    g.fan = gm.d > 0.0f;
-    g.dSize = gm.dSize;
-    g.beamWidth = (double)gm.dSize * (double)gm.effectiveRate;
-    g.d = gm.d;
-    g.beamWidthF = (float)g.beamWidth;
-    g.dF = gm.d;
-    g.invEr = 1.0f / gm.effectiveRate;
-    g.effRate = gm.effectiveRate;
-    p.nb = gm.np < gm.prjFull / 8 + 1 ? gm.np : gm.prjFull / 8 + 1;
-    p.k0 = (g.W % 2 == 0) ? 1 : 0;
-    p.nk = g.fan ? (g.W % 2 == 0 ? g.W - 1 : g.W) : (g.W % 2 == 0 ? g.W / 2 : (g.W + 1) / 2);
+    p.g = make_geo(gm);
+    const Geo &g = p.g;
+    fwd_ray_set(g, &p.nb, &p.k0, &p.nk);
 
     int dev = 0;
-    int st = cuda_error(cudaGetDevice(&dev), "cudaGetDevice");
-    if (st) return st;
+    if ((st = cuda_error(cudaGetDevice(&dev), "cudaGetDevice"))) return st;
     p.device = dev;
-    cudaStream_t s = (cudaStream_t)stream;
 
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     NoAllocSymbols sym;
     if ((st = noalloc_symbols(dev, &sym))) return st;
-    for (int b = 0; b < p.nb; ++b) {
-        const double th = noalloc_view_angle(b, g.P);
-        g_host_view[b].c = cos(th);
-        g_host_view[b].s = sin(th);
-        const bool mirror = b > 0 && (float)b < (float)g.P * 0.125f;
-        for (int j = 0; j < 8; ++j) {
-            const int v = noalloc_view_of(j, b, g.P);
-            g_host_view[b].out[j] = ((j < 4 || mirror) && v < g.np) ? v : -1;
-        }
-    }
-    for (int k = 0; k < g.W; ++k) {
-        DetEntry &e = g_host_det[k];
-        e.t = (double)(k - g.pC) * g.dSize;
-        if (g.fan) {
-            const double bq = sqrt(g.d * g.d + e.t * e.t);
-            e.cB = g.d / bq;
-            e.sB = e.t / bq;
-            e.invbq = (float)(1.0 / bq);
-        } else {
-            e.cB = 1.0;
-            e.sB = 0.0;
-            e.invbq = 0.0f;
-        }
-        e.cBf = (float)e.cB;
-        e.sBf = (float)e.sB;
-        e.pad = 0;
-    }
+    fill_fwd_views(g, p.nb, g_host_view);
+    fill_det_table(g, g_host_det);
     // pageable-memory copies return once the host tables have been staged, so
     // the static host buffers may be refilled by the next call
     if ((st = cuda_error(cudaMemcpyAsync(sym.view, g_host_view, sizeof(FwdView) * (size_t)p.nb,

@@ -26,7 +26,11 @@ extern "C" {
  * return CTPRJ_ERANGE.  All calls share the scratch arrays: calls that overlap
  * on the GPU (other streams, other host threads) race and must be serialised by
  * the caller.  The first call on a device looks up the arrays' device
- * addresses; make it before any stream capture. */
+ * addresses; make it before any stream capture.  Those addresses are kept until
+ * the process exits, so a caller must not reset the device (cudaDeviceReset)
+ * and then call again.  A call on a stream that is being captured returns
+ * CTPRJ_EINVAL: the table uploads read static host buffers that every later
+ * call overwrites. */
 int ctprj_forward_noalloc(const ctprj_geometry *geom, const float *d_img, float *d_sino,
                           void *stream);
 

@@ -12,7 +12,9 @@ package.
   bhc/poissLAlpha.m and bhc/poissLI.m.
 * ``ref``             the reference's own prj/cpuPrj.c and prj/parPrj.c,
   compiled unchanged into ``oracle/_ref`` when the reference sources are
-  present (``make -C oracle ref``); used to pin the restatements.
+  present (``make -C oracle ref REF=<reference>/prj``; the build functions
+  below find the reference through the environment variable
+  IMGRECSRC_REFERENCE); used to pin the restatements.
 
 Geometry arguments are any object with the attributes of the reference's
 ``struct prjConf`` (prj/prj.h:42-57): n, prjWidth, np, prjFull, dSize,
@@ -51,26 +53,38 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
 
 
-def build_ref(ref_prj_dir="/root/reference/prj"):
-    if not os.path.isdir(ref_prj_dir):
+def reference_dir(sub):
+    """<reference>/<sub> where the environment variable IMGRECSRC_REFERENCE
+    names the reference project's root, else None."""
+    root = os.environ.get("IMGRECSRC_REFERENCE")
+    return os.path.join(root, sub) if root else None
+
+
+def build_ref(ref_prj_dir=None):
+    """The reference's own projector sources (<reference>/prj), compiled
+    unchanged into oracle/_ref; False when they are not there."""
+    ref_prj_dir = ref_prj_dir or reference_dir("prj")
+    if not ref_prj_dir or not os.path.isdir(ref_prj_dir):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "ref", "REF=" + ref_prj_dir], check=True)
     return True
 
 
-def build_rwt(ref_rwt_dir="/root/reference/rwt"):
+def build_rwt(ref_rwt_dir=None):
     """The reference's vendored wavelet transform cores (rwt/mdwt_r.c,
     rwt/midwt_r.c), compiled unchanged into oracle/_ref/libref_rwt.so."""
-    if not os.path.isdir(ref_rwt_dir):
+    ref_rwt_dir = ref_rwt_dir or reference_dir("rwt")
+    if not ref_rwt_dir or not os.path.isdir(ref_rwt_dir):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "rwt", "RWT=" + ref_rwt_dir], check=True)
     return True
 
 
-def build_gateways(ref_prj_dir="/root/reference/prj"):
+def build_gateways(ref_prj_dir=None):
     """The reference's own MEX gateways compiled against the engine library
     (oracle/Makefile target `gateways`), for the boundary tests."""
-    if not os.path.isdir(ref_prj_dir):
+    ref_prj_dir = ref_prj_dir or reference_dir("prj")
+    if not ref_prj_dir or not os.path.isdir(ref_prj_dir):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "gateways", "REF=" + ref_prj_dir], check=True)
     return True

@@ -46,9 +46,9 @@ PARPRJ_CASES = [
 
 
 def main():
-    refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/prj"
-    if not oracle.build_ref(refdir):
-        raise SystemExit("reference sources not found at " + refdir)
+    refdir = sys.argv[1] if len(sys.argv) > 1 else oracle.reference_dir("prj")
+    if not refdir or not oracle.build_ref(refdir):
+        raise SystemExit("reference sources not found: pass <reference>/prj or set IMGRECSRC_REFERENCE")
     rng = np.random.default_rng(20240601)
     out = {}
     for ci, (n, W, npv, P, ds, er, d) in enumerate(PROJECTOR_CASES):

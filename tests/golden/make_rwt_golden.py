@@ -35,9 +35,9 @@ CASES = [
 
 
 def main():
-    rwt = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/rwt"
-    if not oracle.build_rwt(rwt):
-        sys.exit("reference rwt sources not found at %s" % rwt)
+    rwt = sys.argv[1] if len(sys.argv) > 1 else oracle.reference_dir("rwt")
+    if not rwt or not oracle.build_rwt(rwt):
+        sys.exit("reference rwt sources not found: pass <reference>/rwt or set IMGRECSRC_REFERENCE")
     rng = np.random.default_rng(20240611)
     out = {}
     for i, (daub, m, n, L) in enumerate(CASES):

@@ -50,3 +50,35 @@ def test_single_process_needs_no_group():
     import bench
     assert bench.max_over_ranks(3.0, None, "cpu") == 3.0
     assert bench.replica_value(1, 2.0e9, 1000.0) == pytest.approx(2.0)
+
+
+def test_gpus_two_starts_two_ranks_itself():
+    """`bench.py --gpus 2` without torchrun's environment launches two ranks
+    (torch.distributed.run, rendezvous on 127.0.0.1) and the line rank 0
+    prints reports both; the host selftest step stands in for the projector."""
+    import json
+    import subprocess
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("WORLD_SIZE", "RANK", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--selftest",
+                        "--steps", "3", "--warmup", "3"], capture_output=True, text=True, env=env,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2
+    assert line["ms_per_step"] >= line["rank_ms"]
+    per_rank = 2 * 256 ** 3 / (line["ms_per_step"] * 1e-3) / 1e9
+    assert line["value"] == pytest.approx(2 * per_rank)
+
+
+def test_rank_count_must_match_gpus():
+    """A run whose torchrun environment holds fewer ranks than --gpus asks for
+    stops instead of reporting a smaller job under the larger name."""
+    import subprocess
+    env = dict(os.environ, WORLD_SIZE="1", RANK="0", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--selftest",
+                        "--steps", "1"], capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode != 0
+    assert "1 ranks started for --gpus 2" in r.stderr

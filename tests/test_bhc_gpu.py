@@ -80,6 +80,32 @@ def test_fused_forward_and_adjoint_match_fp64_oracle(name):
         name, abs(f - fo) / abs(fo), rel(gx.cpu().numpy(), gxo), rel(gI.cpu().numpy(), gIo)))
 
 
+def test_fused_forward_and_adjoint_match_fp64_oracle_at_the_1024_configuration():
+    """The polychromatic model's own configuration: fan 1024^2, 720 views over
+    [0, 2 pi), 1024 detectors, source 2048 px from the isocentre, J = 20,
+    two-material phantom, Poisson counts at I0 = 1e5 of the FP64 oracle's
+    intensity.  f, df/dx and df/dIe against the FP64 oracle (the FP64
+    projector restatement and oracle/bhc_oracle.py, bhc/poissLAlpha.m:1-19 and
+    bhc/poissLI.m:1-27): f within 1e-6 relative, both gradients within 1e-5
+    relative L2."""
+    g = ct.Geometry(1024, 1024, 720, 720, 1.0, 1.0, 2048.0)
+    x, k, Ie, m, Ts = problem(g, J=20, seed=4)
+    pr = ct.Projector(g)
+    model = bhc.BHCModel(pr, k, Ts)
+    dx = torch.from_numpy(x).cuda()
+    dI = torch.from_numpy(Ie).cuda()
+    m32 = m.astype(np.float32)
+    dm = torch.from_numpy(m32).cuda()
+    f = model.forward(dx, dI, dm).item()
+    gx, gI = model.backward()
+    fo, gxo, gIo = oracle_eval(g, x, k, Ie, m32.astype(np.float64), Ts)
+    ef, ex, eI = abs(f - fo) / abs(fo), rel(gx.cpu().numpy(), gxo), rel(gI.cpu().numpy(), gIo)
+    print("bhc fan 1024^2 / 720 views: f rel %.2e, grad_x rel %.2e, grad_Ie rel %.2e" % (ef, ex, eI))
+    assert ef <= 1e-6
+    assert ex < 1e-5
+    assert eI < 1e-5
+
+
 def test_fused_equals_unfused_and_recompute_equals_store():
     g = GEOMS["fan"]
     x, k, Ie, m, Ts = problem(g, J=30, seed=2)
