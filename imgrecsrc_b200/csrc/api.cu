@@ -431,6 +431,23 @@ extern "C" void showSetup(void)
 
 int ctprj_fbp_device(ctprj_plan *plan, const float *d_sino, float *d_img, cudaStream_t s);
 
+// The device address of a host buffer the GPU can write directly (page-locked
+// and mapped, as every cudaHostAlloc / cudaHostRegister buffer is under
+// unified addressing), or NULL for pageable memory.
+static float *mapped_alias(void *host)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? (float *)a.devicePointer : nullptr;
+}
+
+// prj/gpuPrj.cu:899-958: upload the input, run the pass, download the result,
+// return when the result is in the caller's buffer.  When the result buffer is
+// page-locked the kernel writes it directly over the bus as it produces it, so
+// the download overlaps the pass instead of following it.
 extern "C" int gpuPrj(float *img, float *sino, char cmd)
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -442,19 +459,21 @@ extern "C" int gpuPrj(float *img, float *sino, char cmd)
     cudaStream_t s = 0;
     int st;
     if (cmd & FWD_BIT) {
+        float *out = mapped_alias(sino);
         if ((st = cuda_error(cudaMemcpyAsync(g_dimg, img, ib, cudaMemcpyHostToDevice, s), "image upload")) ||
-            (st = ctprj_forward(g_plan, g_dimg, g_dsino, s)) ||
-            (st = cuda_error(cudaMemcpyAsync(sino, g_dsino, sb, cudaMemcpyDeviceToHost, s), "sinogram download")))
+            (st = ctprj_forward(g_plan, g_dimg, out ? out : g_dsino, s)))
             return st;
-    } else if (cmd & BWD_BIT) {
-        if ((st = cuda_error(cudaMemcpyAsync(g_dsino, sino, sb, cudaMemcpyHostToDevice, s), "sinogram upload")) ||
-            (st = ctprj_backward(g_plan, g_dsino, g_dimg, s)) ||
-            (st = cuda_error(cudaMemcpyAsync(img, g_dimg, ib, cudaMemcpyDeviceToHost, s), "image download")))
+        if (!out && (st = cuda_error(cudaMemcpyAsync(sino, g_dsino, sb, cudaMemcpyDeviceToHost, s),
+                                     "sinogram download")))
             return st;
-    } else if (cmd & FBP_BIT) {
+    } else if (cmd & (BWD_BIT | FBP_BIT)) {
+        float *out = mapped_alias(img);
         if ((st = cuda_error(cudaMemcpyAsync(g_dsino, sino, sb, cudaMemcpyHostToDevice, s), "sinogram upload")) ||
-            (st = ctprj_fbp_device(g_plan, g_dsino, g_dimg, s)) ||
-            (st = cuda_error(cudaMemcpyAsync(img, g_dimg, ib, cudaMemcpyDeviceToHost, s), "image download")))
+            (st = (cmd & BWD_BIT) ? ctprj_backward(g_plan, g_dsino, out ? out : g_dimg, s)
+                                  : ctprj_fbp_device(g_plan, g_dsino, out ? out : g_dimg, s)))
+            return st;
+        if (!out && (st = cuda_error(cudaMemcpyAsync(img, g_dimg, ib, cudaMemcpyDeviceToHost, s),
+                                     "image download")))
             return st;
     } else {
         return CTPRJ_OK;   // the reference does nothing for other commands

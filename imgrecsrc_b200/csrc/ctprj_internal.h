@@ -85,10 +85,10 @@ struct BwdParams {
     int zero_axes;            // even n: row 0 and column 0 written as zero
     float scale;              // output scale: FBP PI_f/np/dSize^2, BHC gradient Ts, else 1
     int fast_shadow;          // fan: pixel shadows from the first-order expansion (staged kernel)
+    int win3;                 // staged kernel: three detectors per pixel and view hold every shadow
     const BwdView *view;
     const DetEntry *det;
 };
-
 // One slice of a batch (batch.cu): its plan's parameter blocks and buffers.
 struct BatchSlice {
     FwdParams fp;

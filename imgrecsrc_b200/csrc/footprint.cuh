@@ -43,10 +43,14 @@ __device__ __forceinline__ float trap_cdf(float u, const Footprint &f)
     return fmaf(fmaf(p, p, -r * r), f.iw2, q + r);
 }
 
+// The beam edges' offsets are formed with __fsub_rn: callers pass products as
+// dist or the beam width, and a fused multiply-subtract would round them
+// differently in different kernels (the batched and per-plan launches must
+// give the same bits).
 __device__ __forceinline__ float footprint_weight(float dist, float bw, const Footprint &f)
 {
     const float hb = 0.5f * bw;
-    return f.h * (trap_cdf(hb - dist, f) - trap_cdf(-hb - dist, f));
+    return f.h * (trap_cdf(__fsub_rn(hb, dist), f) - trap_cdf(__fsub_rn(-hb, dist), f));
 }
 
 // The same weight without branches or min/max, every clamp done by the
@@ -85,10 +89,11 @@ __host__ __device__ __forceinline__ FootprintV make_footprint_v(float c, float s
     return q;
 }
 
-// weight for distance D = dist / w and half beam width H = hb / w
+// weight for distance D = dist / w and half beam width H = hb / w (the edge
+// offsets unfused, as in footprint_weight)
 __device__ __forceinline__ float footprint_weight_v(float D, float H, const FootprintV &q)
 {
-    const float v1 = H - D, v2 = -H - D;
+    const float v1 = __fsub_rn(H, D), v2 = __fsub_rn(-H, D);
     const float P1 = __saturatef(q.c1 + v1), R1 = __saturatef(q.c1 - v1);
     const float P2 = __saturatef(q.c1 + v2), R2 = __saturatef(q.c1 - v2);
     const float Q1 = __saturatef(fmaf(v1, q.rho, 0.5f)), Q2 = __saturatef(fmaf(v2, q.rho, 0.5f));

@@ -14,9 +14,15 @@
 // [0, nc) are skipped as in the reference (prj/parPrj.c:170), and also those
 // beyond prjWidth, which the reference would write past its row.
 //
-//  forward   one block per (angle, pixel chunk); the chunk's contributions
-//            accumulate in a shared-memory row (FP64 atomics), then the row is
-//            added to the output view.
+//  forward   one thread per (angle, detector), gathering from a dense copy of
+//            the masked image the pixels whose footprint reaches the detector.
+//            Where the detector's band is closer to the rows than to the
+//            columns (|sin| >= |cos|) they are taken column by column and row
+//            by row -- increasing column-major index, the order in which the
+//            reference sums a sorted mask -- otherwise row by row from a
+//            row-major copy, so that the lanes of a warp (adjacent detectors)
+//            always walk their bands in step.  No atomics: results repeat bit
+//            for bit.
 //  backward  one thread per masked pixel, gathering over angles and detectors
 //            in the reference's order; no atomics.
 #include <cmath>
@@ -30,7 +36,8 @@
 namespace ctprj {
 
 struct ParView {
-    double c, s, height, b1, b2, areaT, areaR, pad;
+    double c, s, height, b1, b2, areaT, areaR;
+    double inv_s, inv_c;   // 1 / s and 1 / c, 0 where zero
 };
 
 struct ParArgs {
@@ -55,11 +62,19 @@ static ParView par_view(double theta)
     v.areaR = v.height * v.b1 * 2;
     v.c = cos(theta * kParPi / 180);
     v.s = sin(theta * kParPi / 180);
-    v.pad = 0;
+    v.inv_s = v.s != 0.0 ? 1.0 / v.s : 0.0;
+    v.inv_c = v.c != 0.0 ? 1.0 / v.c : 0.0;
     return v;
 }
 
 __device__ __forceinline__ double sq(double a) { return a * a; }
+
+// distance of pixel (px, py) from the central ray of angle v (prj/parPrj.c:123),
+// one rounding order for both directions
+__device__ __forceinline__ double par_dist(const ParView &v, int px, int py)
+{
+    return fma((double)py, v.s, (double)px * v.c);
+}
 
 // overlap of the beam of detector k with the footprint centred at dist, by the
 // zones of the beam's two edges (prj/parPrj.c:133-168)
@@ -91,33 +106,86 @@ __device__ __forceinline__ double par_overlap(const ParView &v, double dist, dou
 
 constexpr int kParThreads = 256;
 
-__global__ void __launch_bounds__(kParThreads)
-k_par_forward(const ParArgs a, const double *__restrict__ x, const double *__restrict__ mask,
-              long long npix, double *__restrict__ y)
+// the masked pixel values in a dense nr x nc image, column-major (ximg) and
+// row-major (ximgT), zero elsewhere.  A pixel listed twice in the mask holds
+// the sum of its values; indices outside the image are not projected.
+__global__ void k_par_scatter(const double *__restrict__ x, const double *__restrict__ mask,
+                              long long npix, int nr, int nc, double *__restrict__ ximg,
+                              double *__restrict__ ximgT)
 {
-    extern __shared__ double row[];
-    const int it = blockIdx.x;
-    for (int k = threadIdx.x; k < a.W; k += blockDim.x) row[k] = 0.0;
-    __syncthreads();
-    const ParView v = a.view[it];
-    for (long long i = (long long)blockIdx.y * blockDim.x + threadIdx.x; i < npix;
-         i += (long long)gridDim.y * blockDim.x) {
-        const int m = (int)mask[i];
-        const int px = m / a.nr - a.xC, py = m % a.nr - a.yC;
-        const double dist = px * v.c + py * v.s;
-        const double ub = floor(dist + v.b2 + a.bw / 2 - kParEps);
-        const double lb = ceil(dist - v.b2 - a.bw / 2 + kParEps);
-        const double xi = x[i];
-        for (int k = (int)lb; k <= ub; ++k) {
-            if (k < -a.pC || k + a.pC >= a.nc || k + a.pC >= a.W) continue;
-            const double w = par_overlap(v, dist, (double)k, a.bw);
-            if (w != 0.0) atomicAdd(&row[k + a.pC], w * xi);
+    const long long nimg = (long long)nr * nc;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npix;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long m = (long long)mask[i];
+        if (m >= 0 && m < nimg) {
+            atomicAdd(&ximg[m], x[i]);
+            atomicAdd(&ximgT[(m % nr) * nc + m / nr], x[i]);
         }
     }
-    __syncthreads();
-    double *out = y + (size_t)it * a.W;
-    for (int k = threadIdx.x; k < a.W; k += blockDim.x)
-        if (row[k] != 0.0) atomicAdd(&out[k], row[k]);
+}
+
+// y[it, kk] = (y[it, kk] + sum of w * x over the pixels that reach detector
+// kk) / bw.  The rows a column can contribute are bracketed from
+// |dist - k| <= b2 + bw/2 with a margin; each pixel then takes the reference's
+// own detector range test (prj/parPrj.c:124-125) and weight.
+__global__ void __launch_bounds__(kParThreads)
+k_par_forward(const ParArgs a, const double *__restrict__ ximg, const double *__restrict__ ximgT,
+              double *__restrict__ y)
+{
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)a.np * a.W) return;
+    const int it = (int)(e / a.W), kk = (int)(e % a.W);
+    double acc = y[e];
+    if (kk < a.nc) {   // detectors with k + centre >= nc are skipped (prj/parPrj.c:170)
+        const ParView v = a.view[it];
+        const double k = (double)(kk - a.pC);
+        const double hw = v.b2 + a.bw / 2 + 1e-6;
+        const double ylo = (double)-a.yC, yhi = (double)(a.nr - 1 - a.yC);
+        const double xlo = (double)-a.xC, xhi = (double)(a.nc - 1 - a.xC);
+        // the pixel's own range test and weight (prj/parPrj.c:124-125, :133-168)
+        auto add = [&](int px, int py, double xv) {
+            if (xv == 0.0) return;
+            const double dist = par_dist(v, px, py);
+            const double ub = floor(dist + v.b2 + a.bw / 2 - kParEps);
+            const double lb = ceil(dist - v.b2 - a.bw / 2 + kParEps);
+            if (k < lb || k > ub) return;
+            const double w = par_overlap(v, dist, k, a.bw);
+            if (w != 0.0) acc += w * xv;
+        };
+        if (fabs(v.s) < fabs(v.c)) {
+            // the band is closer to the columns: row by row, a few columns each
+            for (int ry = 0; ry < a.nr; ++ry) {
+                const int py = ry - a.yC;
+                const double ps = (double)py * v.s;
+                double c0 = (k - hw - ps) * v.inv_c, c1 = (k + hw - ps) * v.inv_c;
+                if (c0 > c1) { const double t = c0; c0 = c1; c1 = t; }
+                const int px0 = (int)ceil(fmax(c0, xlo)), px1 = (int)floor(fmin(c1, xhi));
+                const double *row = ximgT + (size_t)ry * a.nc + a.xC;
+                for (int px = px0; px <= px1; ++px) add(px, py, row[px]);
+            }
+            y[e] = acc / a.bw;
+            return;
+        }
+        for (int cx = 0; cx < a.nc; ++cx) {
+            const int px = cx - a.xC;
+            const double pc = (double)px * v.c;
+            double r0, r1;
+            if (v.inv_s != 0.0) {
+                r0 = (k - hw - pc) * v.inv_s;
+                r1 = (k + hw - pc) * v.inv_s;
+                if (r0 > r1) { const double t = r0; r0 = r1; r1 = t; }
+            } else if (fabs(pc - k) <= hw) {
+                r0 = ylo;
+                r1 = yhi;
+            } else {
+                continue;
+            }
+            const int py0 = (int)ceil(fmax(r0, ylo)), py1 = (int)floor(fmin(r1, yhi));
+            const double *col = ximg + (size_t)cx * a.nr + a.yC;
+            for (int py = py0; py <= py1; ++py) add(px, py, col[py]);
+        }
+    }
+    y[e] = acc / a.bw;
 }
 
 __global__ void __launch_bounds__(kParThreads)
@@ -131,7 +199,7 @@ k_par_backward(const ParArgs a, const double *__restrict__ y, const double *__re
     double acc = x[i];
     for (int it = 0; it < a.np; ++it) {
         const ParView &v = a.view[it];
-        const double dist = px * v.c + py * v.s;
+        const double dist = par_dist(v, px, py);
         const double ub = floor(dist + v.b2 + a.bw / 2 - kParEps);
         const double lb = ceil(dist - v.b2 - a.bw / 2 + kParEps);
         const double *rowp = y + (size_t)it * a.W;
@@ -144,22 +212,14 @@ k_par_backward(const ParArgs a, const double *__restrict__ y, const double *__re
     x[i] = acc / a.bw;
 }
 
-__global__ void k_scale(double *__restrict__ v, long long n, double inv)
-{
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x)
-        v[i] /= inv;
-}
-
 static int par_validate(const ctprj_par_conf *c, long long npix)
 {
     if (!c) return set_error(CTPRJ_EINVAL, "NULL configuration");
     if (c->nc < 1 || c->nr < 1 || c->np < 0 || c->prjWidth < 1 || npix < 0 || !(c->bw > 0))
         return set_error(CTPRJ_EINVAL, "invalid parPrj configuration");
-    if ((long long)c->np * c->prjWidth >= (1LL << 31) || npix >= (1LL << 31))
+    if ((long long)c->np * c->prjWidth >= (1LL << 31) || npix >= (1LL << 31) ||
+        (long long)c->nc * c->nr >= (1LL << 31))
         return set_error(CTPRJ_ERANGE, "parPrj sizes exceed 2^31");
-    if ((size_t)c->prjWidth * sizeof(double) > 200 * 1024)
-        return set_error(CTPRJ_ERANGE, "parPrj: prjWidth above %d", (int)(200 * 1024 / sizeof(double)));
     return CTPRJ_OK;
 }
 
@@ -214,23 +274,26 @@ extern "C" int ctprj_par_forward(const ctprj_par_conf *conf, const double *theta
     cudaStream_t s = (cudaStream_t)stream;
     if (conf->np == 0) return CTPRJ_OK;
     ParView *d_view = nullptr;
+    double *d_img = nullptr;
     if ((st = par_table(conf, theta_host, &d_view, s))) return st;
     const ParArgs a = par_args(conf, d_view);
-    const size_t smem = sizeof(double) * (size_t)conf->prjWidth;
-    cudaFuncSetAttribute(k_par_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const long long per = (long long)kParThreads * 8;
-    int chunks = (int)((npix + per - 1) / per);
-    const int target = (4 * sm_count() + conf->np - 1) / conf->np;
-    if (chunks > target) chunks = target;
-    if (chunks < 1) chunks = 1;
-    if (chunks > 65535) chunks = 65535;
-    if (npix > 0) {
-        k_par_forward<<<dim3(conf->np, chunks), kParThreads, smem, s>>>(a, d_x, d_mask, npix, d_y);
-        if ((st = cuda_error(cudaGetLastError(), "parPrj forward"))) return st;
+    const size_t img_elems = (size_t)conf->nc * (size_t)conf->nr, img_bytes = 2 * sizeof(double) * img_elems;
+    if (!(st = cuda_error(cudaMallocAsync((void **)&d_img, img_bytes, s), "parPrj dense image")) &&
+        !(st = cuda_error(cudaMemsetAsync(d_img, 0, img_bytes, s), "parPrj dense image"))) {
+        if (npix > 0) {
+            const long long blocks = (npix + kParThreads - 1) / kParThreads;
+            k_par_scatter<<<(int)(blocks < 8 * sm_count() ? blocks : 8 * sm_count()), kParThreads, 0, s>>>(
+                d_x, d_mask, npix, conf->nr, conf->nc, d_img, d_img + img_elems);
+            st = cuda_error(cudaGetLastError(), "parPrj scatter");
+        }
+        if (!st) {
+            const long long ny = (long long)conf->np * conf->prjWidth;
+            k_par_forward<<<(int)((ny + kParThreads - 1) / kParThreads), kParThreads, 0, s>>>(
+                a, d_img, d_img + img_elems, d_y);
+            st = cuda_error(cudaGetLastError(), "parPrj forward");
+        }
     }
-    const long long ny = (long long)conf->np * conf->prjWidth;
-    k_scale<<<4 * sm_count(), 256, 0, s>>>(d_y, ny, conf->bw);
-    st = cuda_error(cudaGetLastError(), "parPrj scale");
+    if (d_img) cudaFreeAsync(d_img, s);
     cudaFreeAsync(d_view, s);
     return st;
 }

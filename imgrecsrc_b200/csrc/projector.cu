@@ -23,6 +23,7 @@
 // of O(n)); that keeps the projections within 1e-7..1e-6 of the FP64 oracle,
 // where the reference's own FP32 build is 1.5e-5 off on signed inputs.
 // The footprint itself is branch-free (footprint.cuh).
+#include <climits>
 #include <cstdio>
 #include <type_traits>
 
@@ -135,6 +136,75 @@ __device__ __forceinline__ double block_sum(double v, double *red)
     return t;
 }
 
+// Constants of forward ray (base view b, detector k): its direction
+// (cos R, sin R) and offset from the isocentre, the pixel range of each row
+// as xl(y) = Al - y Sl, xr(y) = Ar - y Sr -- the intersections of the two beam
+// edges with the row's band (prj/cpuPrj.c:365-369 parallel, :514-536 fan) --
+// the fan's magnified beam width bwc + (x sinT - y cosT) kbw, and the
+// footprint with its per-pixel steps in ramp units.
+struct FwdRay {
+    double cR, sR, off;
+    float Al, Sl, Ar, Sr;
+    float cT, sT, bwc, kbw;
+    FootprintV fp;
+    float cRw, dhbw;
+};
+
+template <bool FAN>
+__device__ __forceinline__ FwdRay fwd_ray(const FwdParams &p, int b, int k)
+{
+    const Geo &g = p.g;
+    const double cT = p.view[b].c, sT = p.view[b].s;
+    const DetEntry de = p.det[k];
+    const double hbw = 0.5 * g.beamWidth;
+    const double tl = de.t - hbw, tr = de.t + hbw;
+    // every product-sum is an explicit fma, so that no kernel this is inlined
+    // into contracts it differently: the batched and per-plan launches must
+    // give the same bits
+    double cR, sR, off, Al, Sl, Ar, Sr;
+    float bwc = g.beamWidthF, kbw = 0.0f;
+    if (FAN) {
+        const double d = g.d;
+        cR = fma(de.cB, cT, -(de.sB * sT));
+        sR = fma(de.sB, cT, de.cB * sT);
+        off = de.t * de.cB;   // d t / bq
+        const double qxl = fma(tl, cT, d * sT), qyl = fma(-tl, sT, d * cT);
+        const double qxr = fma(tr, cT, d * sT), qyr = fma(-tr, sT, d * cT);
+        Al = fma(qxl > 0 ? -0.5 : 0.5, qxl, d * tl) / qyl;
+        Sl = qxl / qyl;
+        Ar = fma(qxr > 0 ? 0.5 : -0.5, qxr, d * tr) / qyr;
+        Sr = qxr / qyr;
+        const double bwcd = g.beamWidth * de.cB;
+        bwc = (float)bwcd;
+        kbw = (float)(bwcd / d);
+    } else {
+        cR = cT;
+        sR = sT;
+        off = de.t;
+        Al = fma(-0.5, sT, tl) / cT;
+        Sl = sT / cT;
+        Ar = fma(0.5, sT, tr) / cT;
+        Sr = Sl;
+    }
+    FwdRay r;
+    r.cR = cR;
+    r.sR = sR;
+    r.off = off;
+    r.Al = (float)Al;
+    r.Sl = (float)Sl;
+    r.Ar = (float)Ar;
+    r.Sr = (float)Sr;
+    r.cT = (float)cT;
+    r.sT = (float)sT;
+    r.bwc = bwc;
+    r.kbw = kbw;
+    const float dhb = FAN ? 0.5f * r.sT * kbw : 0.0f;   // half beam width step per pixel
+    r.fp = make_footprint_v((float)cR, (float)sR);
+    r.cRw = (float)cR * r.fp.iw;
+    r.dhbw = dhb * r.fp.iw;
+    return r;
+}
+
 // The rays of one forward block: V adjacent base views (one per warp) x 32
 // adjacent detectors; block (bx, by) of the per-plan grid.  Returns this
 // thread's Poisson terms in polychromatic mode.
@@ -156,48 +226,31 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
             else sino[(size_t)v * g.W] = 0.0f;
         }
 
-    if (b < p.nb && r < p.nk) {
-        const int k = p.k0 + r;
-        const double cT = p.view[b].c, sT = p.view[b].s;
-        const DetEntry de = p.det[k];
-        const double hbw = 0.5 * g.beamWidth;
-        const double tl = de.t - hbw, tr = de.t + hbw;
-
-        // Ray direction (cos R, sin R), its offset from the isocentre, and the
-        // pixel range of each row as xl(y) = Al - y Sl, xr(y) = Ar - y Sr: the
-        // intersections of the two beam edges with the row's band
-        // (prj/cpuPrj.c:365-369 parallel, :514-536 fan).
-        double cR, sR, off, Al, Sl, Ar, Sr;
-        float bwc = g.beamWidthF, kbw = 0.0f;
-        if (FAN) {
-            const double d = g.d;
-            cR = de.cB * cT - de.sB * sT;
-            sR = de.sB * cT + de.cB * sT;
-            off = de.t * de.cB;   // d t / bq
-            const double qxl = tl * cT + d * sT, qyl = -tl * sT + d * cT;
-            const double qxr = tr * cT + d * sT, qyr = -tr * sT + d * cT;
-            Al = (d * tl - (qxl > 0 ? 0.5 : -0.5) * qxl) / qyl;
-            Sl = qxl / qyl;
-            Ar = (d * tr + (qxr > 0 ? 0.5 : -0.5) * qxr) / qyr;
-            Sr = qxr / qyr;
-            // magnified beam width at pixel (x, y): bwc + (x sinT - y cosT) bwc / d
-            const double bwcd = g.beamWidth * de.cB;
-            bwc = (float)bwcd;
-            kbw = (float)(bwcd / d);
-        } else {
-            cR = cT;
-            sR = sT;
-            off = de.t;
-            Al = (tl - 0.5 * sT) / cT;
-            Sl = sT / cT;
-            Ar = (tr + 0.5 * sT) / cT;
-            Sr = Sl;
+    // The window a warp marches with (below) is the widest any of its rays
+    // needs: xr - xl is affine in y, so a ray's widest run is at the first or
+    // the last row.  Every lane of the (full) warp takes part in the maximum,
+    // lanes without a ray with 0, so the choice depends on the warp's rays
+    // alone and a batched launch makes the same one.
+    const bool live = b < p.nb && r < p.nk;
+    const int k = p.k0 + r;
+    FwdRay ray = {};
+    int wcode = 0;   // 3 / 4: window of 3 / 4 pixels; 5: bounded range loop
+    if (live) {
+        ray = fwd_ray<FAN>(p, b, k);
+        wcode = 5;
+        if (MODE != kModeCount && g.half >= 3) {
+            const float wa = ray.Ar - ray.Al, ws = ray.Sr - ray.Sl, hf = (float)g.half;
+            const float wmax = fmaxf(fabsf(fmaf(-hf, ws, wa)), fabsf(fmaf(hf, ws, wa)));
+            wcode = wmax < 1.95f ? 3 : (wmax < 2.95f ? 4 : 5);
         }
-        const float Alf = (float)Al, Slf = (float)Sl, Arf = (float)Ar, Srf = (float)Sr;
-        const float cRf = (float)cR, cTf = (float)cT, sTf = (float)sT;
-        const float dhb = FAN ? 0.5f * sTf * kbw : 0.0f;   // half beam width step per pixel
-        const FootprintV fp = make_footprint_v(cRf, (float)sR);
-        const float cRw = cRf * fp.iw, dhbw = dhb * fp.iw;   // per-pixel steps in ramp units
+    }
+    wcode = __reduce_max_sync(0xffffffffu, wcode);
+    if (live) {
+        const double cR = ray.cR, sR = ray.sR, off = ray.off;
+        const float Alf = ray.Al, Slf = ray.Sl, Arf = ray.Ar, Srf = ray.Sr;
+        const float cTf = ray.cT, sTf = ray.sT, bwc = ray.bwc, kbw = ray.kbw;
+        const FootprintV fp = ray.fp;
+        const float cRw = ray.cRw, dhbw = ray.dhbw;
 
         const int half = g.half;
         float S[8];
@@ -295,11 +348,74 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
                 accumulate(footprint_weight_v(D, H, fp), __ldg(q + x), __ldg(q - x));
             }
         };
+        // The fixed-window march (plain and polychromatic modes).  Where a
+        // ray's run across a row is always narrower than 1.95 (2.95) pixels,
+        // the pixels of the run lie within the 3 (4) centred on the ray's
+        // crossing xc = (xl + xr) / 2: they are summed straight, without the
+        // run's bounds.  A pixel of the window outside the run lies beyond
+        // the beam and adds a weight of exactly zero (for fan beams: below
+        // 1e-7 within ~1e-4 pixel of a run edge, where the footprint and the
+        // beam edges differ).  The window is chosen per warp (the widest any
+        // of its rays needs), so the warp stays converged.
+        const float Acf = 0.5f * (Alf + Arf), Scf = 0.5f * (Slf + Srf);
+        auto march_win = [&](const int y, const float4 *__restrict__ q, auto neg, auto wn) {
+            constexpr bool NEG = decltype(neg)::value;
+            constexpr int WN = decltype(wn)::value;
+            const float yf = (float)y;
+            const float xc = fmaf(-yf, Scf, Acf);
+            // rows whose run misses the image (the run lies within xc +- 1.5)
+            if (xc < -(float)half - 2.0f || xc > (float)half + 2.0f) return;
+            int xs = (WN == 3 ? __float2int_rn(xc) : __float2int_rd(xc)) - 1;
+            xs = min(max(xs, -half), half - (WN - 1));
+            const float r0 = (float)fma((double)xs, cR, fma((double)y, sR, -off)) * fp.iw;
+            const float hb0 = (FAN ? 0.5f * fmaf(fmaf((float)xs, sTf, -yf * cTf), kbw, bwc)
+                                   : 0.5f * g.beamWidthF) * fp.iw;
+            float4 pp[WN], pm[WN];
+#pragma unroll
+            for (int j = 0; j < WN; ++j) {
+                pp[j] = __ldg(q + xs + j);
+                pm[j] = __ldg(q - xs - j);
+            }
+#pragma unroll
+            for (int j = 0; j < WN; ++j) {
+                const float D = fmaf((float)j, cRw, r0);
+                const float H = FAN ? fmaf((float)j, dhbw, hb0) : hb0;
+                const float w = footprint_weight_v(D, H, fp);
+                const float ap = NEG ? pp[j].y : pp[j].x, am = NEG ? pm[j].y : pm[j].x;
+                const float bp = NEG ? pp[j].x : pp[j].y, bm = NEG ? pm[j].x : pm[j].y;
+                const float cp = NEG ? pp[j].w : pp[j].z, cm = NEG ? pm[j].w : pm[j].z;
+                const float dp = NEG ? pp[j].z : pp[j].w, dm = NEG ? pm[j].z : pm[j].w;
+                S[0] = fmaf(w, ap, S[0]);
+                S[6] = fmaf(w, am, S[6]);
+                S[4] = fmaf(w, bp, S[4]);
+                S[2] = fmaf(w, bm, S[2]);
+                S[5] = fmaf(w, cp, S[5]);
+                S[3] = fmaf(w, cm, S[3]);
+                S[1] = fmaf(w, dp, S[1]);
+                S[7] = fmaf(w, dm, S[7]);
+            }
+        };
         {
             const float4 *q = quad + (size_t)half * QW + half;   // row |y| = half, x = 0
-            for (int y = half; y >= 0; --y, q -= QW) march_row(y, q, std::false_type{});
+            if (wcode == 3) {
+                for (int y = half; y >= 0; --y, q -= QW)
+                    march_win(y, q, std::false_type{}, std::integral_constant<int, 3>{});
+            } else if (wcode == 4) {
+                for (int y = half; y >= 0; --y, q -= QW)
+                    march_win(y, q, std::false_type{}, std::integral_constant<int, 4>{});
+            } else {
+                for (int y = half; y >= 0; --y, q -= QW) march_row(y, q, std::false_type{});
+            }
             q = quad + (size_t)QW + half;                          // row |y| = 1
-            for (int y = -1; y >= -half; --y, q += QW) march_row(y, q, std::true_type{});
+            if (wcode == 3) {
+                for (int y = -1; y >= -half; --y, q += QW)
+                    march_win(y, q, std::true_type{}, std::integral_constant<int, 3>{});
+            } else if (wcode == 4) {
+                for (int y = -1; y >= -half; --y, q += QW)
+                    march_win(y, q, std::true_type{}, std::integral_constant<int, 4>{});
+            } else {
+                for (int y = -1; y >= -half; --y, q += QW) march_row(y, q, std::true_type{});
+            }
         }
 
         // Scatter to the eight symmetric views (prj/cpuPrj.c:577-615); parallel
@@ -368,6 +484,260 @@ k_forward(const FwdParams p, const float4 *__restrict__ quad, float *__restrict_
     }
 }
 
+#if CTPRJ_FWD_STAGE
+// -------------------------------------------- forward, staged by bulk copies
+//
+// Build-time variant (CTPRJ_FWD_STAGE=1), measured against k_forward.  The
+// block's rays read the quad-image rows of a chunk of kStRows rows from shared
+// memory: one thread brings the row segments in with bulk asynchronous copies
+// (cp.async.bulk, completion counted on an mbarrier), double-buffered so that
+// the copies of chunk c + 1 are in flight while chunk c is summed.  A segment
+// is the union of the block's pixel windows over the chunk's rows, on the +x
+// side and its mirror; a chunk whose union exceeds kStCols pixels is read from
+// global memory instead, and so are warps whose rays need the range loop.
+// Plain mode only.  Waits are bounded (%globaltimer, 1 s): past it the block
+// records the timeout in g_fwd_stage_timeout, writes NaN to its outputs and
+// returns.
+
+#ifndef CTPRJ_FWD_STAGE_ROWS
+#define CTPRJ_FWD_STAGE_ROWS 4
+#endif
+constexpr int kStRows = CTPRJ_FWD_STAGE_ROWS;
+constexpr int kStCols = 128;
+
+struct FwdStage {
+    float4 buf[2][kStRows][2][kStCols];   // [buffer][row][+x side, -x side][pixel]
+    unsigned long long bar[2];
+    int lo[2], hi[2];                      // staged pixels [lo, hi] of each buffer; hi < lo: none
+    int wlo[kFwdViews], whi[kFwdViews];
+};
+
+__device__ int g_fwd_stage_timeout;
+
+__device__ __forceinline__ unsigned long long stage_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *ptr)
+{
+    return (unsigned)__cvta_generic_to_shared(ptr);
+}
+
+// true when the phase of parity `ph` of barrier `bar` completed within 1 s
+__device__ __forceinline__ bool stage_wait(unsigned long long *bar, unsigned ph)
+{
+    const unsigned a = smem_u32(bar);
+    const unsigned long long t0 = stage_ns();
+    for (;;) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(a), "r"(ph) : "memory");
+        if (done) return true;
+        if (stage_ns() - t0 > 1000000000ull) return false;
+    }
+}
+
+template <bool FAN>
+__global__ void __launch_bounds__(kFwdThreads, CTPRJ_FWD_MINBLOCKS)
+k_forward_staged(const FwdParams p, const float4 *__restrict__ quad, float *__restrict__ sino)
+{
+    __shared__ __align__(128) FwdStage st;
+    const Geo &g = p.g;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = blockIdx.x * kFwdViews + warp;
+    const int r = blockIdx.y * 32 + lane;
+    const bool live = b < p.nb && r < p.nk;
+    if (p.zero_col0 && blockIdx.x == 0 && blockIdx.y == 0)
+        for (int v = threadIdx.x; v < g.np; v += blockDim.x) sino[(size_t)v * g.W] = 0.0f;
+    const int half = g.half, QW = 2 * half + 1;
+    const int k = p.k0 + r;
+    FwdRay ray = {};
+    int wcode = 0;   // 0: no ray, 3 / 4: window, 5: range loop (global reads)
+    if (live) {
+        ray = fwd_ray<FAN>(p, b, k);
+        const float wa = ray.Ar - ray.Al, ws = ray.Sr - ray.Sl;
+        const float wmax = fmaxf(fabsf(fmaf(-(float)half, ws, wa)), fabsf(fmaf((float)half, ws, wa)));
+        wcode = half < 3 ? 5 : (wmax < 1.95f ? 3 : (wmax < 2.95f ? 4 : 5));
+    }
+    wcode = __reduce_max_sync(0xffffffffu, wcode);
+    const float Acf = 0.5f * (ray.Al + ray.Ar), Scf = 0.5f * (ray.Sl + ray.Sr);
+    // the window start of this lane's ray at row y (window rays only)
+    auto wstart = [&](int y) {
+        const float xc = fmaf(-(float)y, Scf, Acf);
+        const int xs = (wcode == 3 ? __float2int_rn(xc) : __float2int_rd(xc)) - 1;
+        return min(max(xs, -half), half - (wcode - 1));
+    };
+    const int steps = 2 * half + 1;               // rows y = half - m, m = 0 .. 2 half
+    const int nchunks = (steps + kStRows - 1) / kStRows;
+    // this warp's union of windows over chunk c, then the block's, into buffer c & 1
+    auto plan_chunk = [&](int c) {
+        int lo = INT_MAX, hi = INT_MIN;
+        if (live && (wcode == 3 || wcode == 4)) {
+            const int m0 = c * kStRows, m1 = min(m0 + kStRows, steps) - 1;
+            const int a0 = wstart(half - m0), a1 = wstart(half - m1);
+            lo = min(a0, a1);
+            hi = max(a0, a1) + wcode - 1;
+        }
+        lo = __reduce_min_sync(0xffffffffu, lo);
+        hi = __reduce_max_sync(0xffffffffu, hi);
+        if (lane == 0) {
+            st.wlo[warp] = lo;
+            st.whi[warp] = hi;
+        }
+    };
+    auto issue_chunk = [&](int c) {   // thread 0, after a block barrier
+        const int bc = c & 1;
+        int lo = INT_MAX, hi = INT_MIN;
+        for (int w = 0; w < kFwdViews; ++w) {
+            lo = min(lo, st.wlo[w]);
+            hi = max(hi, st.whi[w]);
+        }
+        if (hi < lo || hi - lo + 1 > kStCols) {
+            st.lo[bc] = 1;
+            st.hi[bc] = 0;
+            return;
+        }
+        st.lo[bc] = lo;
+        st.hi[bc] = hi;
+        const int m0 = c * kStRows, nr = min(kStRows, steps - m0);
+        const unsigned bytes = (unsigned)(hi - lo + 1) * 16u;
+        const unsigned bar = smem_u32(&st.bar[bc]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     :: "r"(bar), "r"(bytes * 2u * (unsigned)nr) : "memory");
+        for (int i = 0; i < nr; ++i) {
+            const int y = half - (m0 + i), row = y < 0 ? -y : y;
+            const float4 *src = quad + (size_t)row * QW + half;
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(smem_u32(&st.buf[bc][i][0][0])), "l"(src + lo), "r"(bytes), "r"(bar)
+                         : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(smem_u32(&st.buf[bc][i][1][0])), "l"(src - hi), "r"(bytes), "r"(bar)
+                         : "memory");
+        }
+    };
+
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&st.bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&st.bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    plan_chunk(0);
+    __syncthreads();
+    if (threadIdx.x == 0) issue_chunk(0);
+
+    float S[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) S[j] = 0.0f;
+    unsigned ph[2] = {0u, 0u};
+    bool failed = false;
+    for (int c = 0; c < nchunks; ++c) {
+        const int bc = c & 1;
+        if (c + 1 < nchunks) plan_chunk(c + 1);
+        // chunk c - 1 read; windows of chunk c + 1 visible; a wait that timed
+        // out in any thread ends the march of the whole block
+        if (__syncthreads_or(failed)) {
+            failed = true;
+            break;
+        }
+        if (threadIdx.x == 0 && c + 1 < nchunks) issue_chunk(c + 1);
+        const int lo = st.lo[bc], hi = st.hi[bc];
+        const bool staged = lo <= hi;
+        if (staged) {
+            if (!stage_wait(&st.bar[bc], ph[bc])) {
+                failed = true;
+                continue;
+            }
+            ph[bc] ^= 1u;
+        }
+        if (!live) continue;
+        const int m0 = c * kStRows, nr = min(kStRows, steps - m0);
+        for (int i = 0; i < nr; ++i) {
+            const int y = half - (m0 + i), row = y < 0 ? -y : y;
+            const bool neg = y < 0;
+            const float4 *q = quad + (size_t)row * QW + half;
+            const float yf = (float)y;
+            if (wcode == 5) {
+                // range loop from global memory (prj/cpuPrj.c:365-369, :514-536 ranges)
+                const int x0 = max(__float2int_rn(fmaf(-yf, ray.Sl, ray.Al)), -half);
+                const int x1 = min(__float2int_rn(fmaf(-yf, ray.Sr, ray.Ar)), half);
+                for (int x = x0; x <= x1; ++x) {
+                    const float D = (float)fma((double)x, ray.cR, fma((double)y, ray.sR, -ray.off)) * ray.fp.iw;
+                    const float H = (FAN ? 0.5f * fmaf(fmaf((float)x, ray.sT, -yf * ray.cT), ray.kbw, ray.bwc)
+                                         : 0.5f * g.beamWidthF) * ray.fp.iw;
+                    const float w = footprint_weight_v(D, H, ray.fp);
+                    const float4 pp = __ldg(q + x), pm = __ldg(q - x);
+                    S[0] = fmaf(w, neg ? pp.y : pp.x, S[0]);
+                    S[6] = fmaf(w, neg ? pm.y : pm.x, S[6]);
+                    S[4] = fmaf(w, neg ? pp.x : pp.y, S[4]);
+                    S[2] = fmaf(w, neg ? pm.x : pm.y, S[2]);
+                    S[5] = fmaf(w, neg ? pp.w : pp.z, S[5]);
+                    S[3] = fmaf(w, neg ? pm.w : pm.z, S[3]);
+                    S[1] = fmaf(w, neg ? pp.z : pp.w, S[1]);
+                    S[7] = fmaf(w, neg ? pm.z : pm.w, S[7]);
+                }
+                continue;
+            }
+            const float xc = fmaf(-yf, Scf, Acf);
+            if (xc < -(float)half - 2.0f || xc > (float)half + 2.0f) continue;
+            const int xs = wstart(y);
+            const float r0 = (float)fma((double)xs, ray.cR, fma((double)y, ray.sR, -ray.off)) * ray.fp.iw;
+            const float hb0 = (FAN ? 0.5f * fmaf(fmaf((float)xs, ray.sT, -yf * ray.cT), ray.kbw, ray.bwc)
+                                   : 0.5f * g.beamWidthF) * ray.fp.iw;
+            // the window's pixels, unrolled for the warp's window width
+            auto row_sum = [&](auto wn) {
+                constexpr int WN = decltype(wn)::value;
+                float4 pp[WN], pm[WN];
+#pragma unroll
+                for (int j = 0; j < WN; ++j) {
+                    pp[j] = staged ? st.buf[bc][i][0][xs + j - lo] : __ldg(q + xs + j);
+                    pm[j] = staged ? st.buf[bc][i][1][hi - xs - j] : __ldg(q - xs - j);
+                }
+#pragma unroll
+                for (int j = 0; j < WN; ++j) {
+                    const float D = fmaf((float)j, ray.cRw, r0);
+                    const float H = FAN ? fmaf((float)j, ray.dhbw, hb0) : hb0;
+                    const float w = footprint_weight_v(D, H, ray.fp);
+                    S[0] = fmaf(w, neg ? pp[j].y : pp[j].x, S[0]);
+                    S[6] = fmaf(w, neg ? pm[j].y : pm[j].x, S[6]);
+                    S[4] = fmaf(w, neg ? pp[j].x : pp[j].y, S[4]);
+                    S[2] = fmaf(w, neg ? pm[j].x : pm[j].y, S[2]);
+                    S[5] = fmaf(w, neg ? pp[j].w : pp[j].z, S[5]);
+                    S[3] = fmaf(w, neg ? pm[j].w : pm[j].z, S[3]);
+                    S[1] = fmaf(w, neg ? pp[j].z : pp[j].w, S[1]);
+                    S[7] = fmaf(w, neg ? pm[j].z : pm[j].w, S[7]);
+                }
+            };
+            if (wcode == 3) row_sum(std::integral_constant<int, 3>{});
+            else row_sum(std::integral_constant<int, 4>{});
+        }
+    }
+    failed = __syncthreads_or(failed);
+    if (failed) {
+        if (threadIdx.x == 0) atomicExch(&g_fwd_stage_timeout, 1);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) S[j] = __int_as_float(0x7fc00000);
+    }
+    if (!live) return;
+    const int pC = g.pC;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int v = p.view[b].out[j];
+        if (v < 0) continue;
+        const int det = j < 4 ? k : 2 * pC - k;
+        const int det2 = 2 * pC - det;
+        const size_t row = (size_t)v * g.W;
+        sino[row + det] = S[j] / g.effRate;
+        if (!FAN) sino[row + det2] = S[j ^ 2] / g.effRate;
+    }
+}
+#endif
+
 static FwdParams fwd_params(const ctprj_plan *pl)
 {
     FwdParams p;
@@ -403,8 +773,13 @@ int launch_forward(const ctprj_plan *pl, const float4 *quad, float *sino,
         if (fan) k_forward<true, kModeCount><<<grid, block, 0, s>>>(p, quad, sino, counter);
         else k_forward<false, kModeCount><<<grid, block, 0, s>>>(p, quad, sino, counter);
     } else {
+#if CTPRJ_FWD_STAGE
+        if (fan) k_forward_staged<true><<<grid, block, 0, s>>>(p, quad, sino);
+        else k_forward_staged<false><<<grid, block, 0, s>>>(p, quad, sino);
+#else
         if (fan) k_forward<true, kModePlain><<<grid, block, 0, s>>>(p, quad, sino, counter);
         else k_forward<false, kModePlain><<<grid, block, 0, s>>>(p, quad, sino, counter);
+#endif
     }
     return cuda_error(cudaGetLastError(), "forward launch");
 }
@@ -683,7 +1058,15 @@ struct TiledSmem {
 };
 
 // One tile of the staged backprojection (all threads of the block take part).
-template <bool FAN, bool FBP, int SEG, int VB>
+// WIN3: every pixel shadow of the plan is narrower than 1.9 detectors (the
+// plan's bound), so the detectors a pixel reaches in a view always lie within
+// the three centred on the projection of its centre: those three are summed
+// straight, without the per-pixel shadow range.  A detector of the three that
+// the reference's range rule (prj/cpuPrj.c:218-244) leaves out lies beyond the
+// pixel's footprint and adds a weight of exactly zero, except within ~1e-4
+// detector of a shadow edge, where the footprint and the exact corner shadow
+// differ and the weight is below 1e-7.
+template <bool FAN, bool FBP, int SEG, int VB, bool WIN3>
 __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                                               const float *__restrict__ sino,
                                               float *__restrict__ img,
@@ -706,8 +1089,11 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     int tx, ty;
     decode_tile(tile, tx, ty);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int x = tx * kBwdTile + (int)(threadIdx.x % kBwdTile);
-    const int y = ty * kBwdTile + (int)(threadIdx.x / kBwdTile);
+    // a warp takes an 8 x 4 block of the tile: compact blocks project onto
+    // fewer staged detectors than 16 x 2 rows, so each shared-memory read of
+    // a warp touches fewer distinct entries
+    const int x = tx * kBwdTile + ((warp & 1) << 3) + (lane & 7);
+    const int y = ty * kBwdTile + ((warp >> 1) << 2) + (lane >> 3);
     const bool valid = x <= g.half && y <= x;
     const int nimg = (y == 0 || y == x) ? 4 : 8;
     const double xc = tx * kBwdTile + 0.5 * (kBwdTile - 1), yc = ty * kBwdTile + 0.5 * (kBwdTile - 1);
@@ -795,6 +1181,54 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                 const float du = fmaf(dx, t.cT, dy * t.sT);
                 const float dv = fmaf(dy, t.cT, -dx * t.sT);
                 const float u = t.ucf + du;
+                if (WIN3 && t.nseg >= 3) {   // t.nseg is the same for the whole block
+                    const float qe = FAN ? t.qec - dv : 0.0f;
+                    // the detector under the pixel centre, in staged units
+                    const float tc = FAN ? __fdividef(dFs * u, qe) : u * invdS;
+                    const int k0 = min(max(__float2int_rn(tc) - 1 - t.klo, 0), t.nseg - 3);
+                    const float fbpw = FBP ? __fdividef(g.dF, qe) * __fdividef(g.dF, qe) : 1.0f;
+                    const FootprintV fpar = FAN ? FootprintV{} : pfs[iv];
+                    const float duw = FAN ? 0.0f : du * fpar.iw, Hpar = FAN ? 0.0f : hbpar * fpar.iw;
+                    float w[3];
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        const float4 a = ra[iv][k0 + q];
+                        if (FAN) {
+                            const float D = fmaf(a.y, du, fmaf(a.z, dv, a.x));
+                            const float4 b = rb[FAN ? iv : 0][FAN ? k0 + q : 0];
+                            const FootprintV f = {b.x, b.y, b.z, b.w, 0.0f};
+                            w[q] = footprint_weight_v(D, qe * a.w, f);
+                            if (FBP) w[q] *= fbpw;
+                        } else {
+                            w[q] = footprint_weight_v(a.x + duw, Hpar, fpar);
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        const float4 p0 = seg[iv][0][k0 + q], p1 = seg[iv][1][k0 + q];
+                        S[0] = fmaf(w[q], p0.x, S[0]);
+                        S[1] = fmaf(w[q], p0.y, S[1]);
+                        S[2] = fmaf(w[q], p0.z, S[2]);
+                        S[3] = fmaf(w[q], p0.w, S[3]);
+                        S[4] = fmaf(w[q], p1.x, S[4]);
+                        S[5] = fmaf(w[q], p1.y, S[5]);
+                        S[6] = fmaf(w[q], p1.z, S[6]);
+                        S[7] = fmaf(w[q], p1.w, S[7]);
+                        if (!FAN) {
+                            const float4 r0 = seg2[FAN ? 0 : iv][0][FAN ? 0 : k0 + q];
+                            const float4 r1 = seg2[FAN ? 0 : iv][1][FAN ? 0 : k0 + q];
+                            S[0] = fmaf(w[q], r0.x, S[0]);
+                            S[1] = fmaf(w[q], r0.y, S[1]);
+                            S[2] = fmaf(w[q], r0.z, S[2]);
+                            S[3] = fmaf(w[q], r0.w, S[3]);
+                            S[4] = fmaf(w[q], r1.x, S[4]);
+                            S[5] = fmaf(w[q], r1.y, S[5]);
+                            S[6] = fmaf(w[q], r1.z, S[6]);
+                            S[7] = fmaf(w[q], r1.w, S[7]);
+                        }
+                    }
+                    continue;
+                }
                 float tlo, thi, qe = 0.0f;
                 if (FAN) {
                     // the pixel's corner shadows (prj/cpuPrj.c:218-244), in
@@ -806,7 +1240,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                         // corner i at (u + du_i, qe + dq_i): t_i = K (u + du_i) / (1 + r dq_i)
                         // ~ K (u + du_i - rho dq_i - r du_i dq_i), K = d r, rho = r u; the
                         // corners pair up as u + c +- a1 and u - c +- a2
-                        const float r = __fdividef(1.0f, qe), rho = r * u, c = r * t.AB;
+                        const float r = __fdividef(1.0f, qe), rho = r * u, c = __fmul_rn(r, t.AB);
                         const float a1 = fabsf(fmaf(rho, B, A)), a2 = fabsf(fmaf(-rho, A, B));
                         const float K = dFs * r;
                         tlo = K * (u + fminf(c - a1, -c - a2));
@@ -880,12 +1314,24 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     if (valid) write_octant(p, img, x, y, nimg, S);
 }
 
-template <bool FAN, bool FBP, int SEG, int VB>
+template <bool FAN, bool FBP, int SEG, int VB, bool WIN3>
 __global__ void __launch_bounds__(kBwdTile * kBwdTile, CTPRJ_BWD_MINBLOCKS)
 k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
 {
     __shared__ TiledSmem<FAN, SEG, VB> sm;
-    backward_tile<FAN, FBP, SEG, VB>(p, blockIdx.x, sino, img, sm);
+    backward_tile<FAN, FBP, SEG, VB, WIN3>(p, blockIdx.x, sino, img, sm);
+}
+
+// upper bound of a pixel's shadow width in detectors, or 0 where none holds
+// (a fan source inside or next to the image)
+static double shadow_width_bound(const Geo &g)
+{
+    const double s2 = 1.4142135623730951;
+    if (!g.fan) return s2 / g.dSize;
+    const double R = (g.half + 1.0) * s2, d = g.d;
+    if (!(d > 2.0 * R)) return 0.0;
+    const double tg = R / (d - R);
+    return s2 * d / (d - R) * (1.0 + tg * tg) / g.dSize;
 }
 
 static BwdParams bwd_params(const ctprj_plan *pl, int fbp, float scale)
@@ -916,6 +1362,17 @@ static BwdParams bwd_params(const ctprj_plan *pl, int fbp, float scale)
             p.fast_shadow = K * (h + 1.0) * r * r * 0.5 <= 1e-4;
         }
     }
+    // Widest pixel shadow, in detectors: a unit pixel spans at most sqrt(2)
+    // across any ray; a fan magnifies that by d / qe <= d / (d - R) at the
+    // pixel nearest the source (R: the image corner's distance from the
+    // isocentre) and the detector's obliquity adds 1 + tan^2 of the fan
+    // angle, tan <= R / (d - R).  Below 1.9 detectors the three detectors
+    // centred on a pixel's projection hold its whole shadow.  A beam wider than
+    // the detector pitch (effectiveRate > 1) also reaches detectors outside the
+    // shadow, which the reference's range rule leaves out: such plans keep the
+    // per-pixel range.
+    const double width = shadow_width_bound(pl->g);
+    p.win3 = width > 0.0 && width <= 1.9 && pl->g.effRate <= 1.0f;
     return p;
 }
 
@@ -938,6 +1395,19 @@ int backward_max_span(const ctprj_plan *pl, int *max_span)
     return st;
 }
 
+template <int SEG, int VB, bool WIN3>
+static void launch_tiled(const BwdParams &p, bool fan, int fbp, dim3 grid, dim3 block,
+                         const float *sino, float *img, cudaStream_t s)
+{
+    if (fan) {
+        if (fbp) k_backward_tiled<true, true, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
+        else k_backward_tiled<true, false, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
+    } else {
+        if (fbp) k_backward_tiled<false, true, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
+        else k_backward_tiled<false, false, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
+    }
+}
+
 int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp,
                     unsigned long long *counter, cudaStream_t s, float scale)
 {
@@ -957,21 +1427,11 @@ int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp
             else k_backward<false, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
         }
     } else if (pl->bwd_seg <= 32) {
-        if (fan) {
-            if (fbp) k_backward_tiled<true, true, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
-            else k_backward_tiled<true, false, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
-        } else {
-            if (fbp) k_backward_tiled<false, true, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
-            else k_backward_tiled<false, false, 32, 16><<<grid, block, 0, s>>>(p, sino, img);
-        }
+        if (p.win3) launch_tiled<32, 16, true>(p, fan, fbp, grid, block, sino, img, s);
+        else launch_tiled<32, 16, false>(p, fan, fbp, grid, block, sino, img, s);
     } else {
-        if (fan) {
-            if (fbp) k_backward_tiled<true, true, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
-            else k_backward_tiled<true, false, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
-        } else {
-            if (fbp) k_backward_tiled<false, true, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
-            else k_backward_tiled<false, false, 64, 8><<<grid, block, 0, s>>>(p, sino, img);
-        }
+        if (p.win3) launch_tiled<64, 8, true>(p, fan, fbp, grid, block, sino, img, s);
+        else launch_tiled<64, 8, false>(p, fan, fbp, grid, block, sino, img, s);
     }
     return cuda_error(cudaGetLastError(), "backward launch");
 }
@@ -1043,6 +1503,21 @@ constexpr size_t tiled_smem_bytes()
                : sizeof(TiledSmem<false, SEG, VB>);
 }
 
+// one staged tile of a batch slice, with the slice's own window choice
+template <int SEG, int VB>
+__device__ __forceinline__ void batch_tile(const BatchSlice &sl, int tile, unsigned char *raw)
+{
+    if (sl.bp.g.fan) {
+        auto &sm = *reinterpret_cast<TiledSmem<true, SEG, VB> *>(raw);
+        if (sl.bp.win3) backward_tile<true, false, SEG, VB, true>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+        else backward_tile<true, false, SEG, VB, false>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+    } else {
+        auto &sm = *reinterpret_cast<TiledSmem<false, SEG, VB> *>(raw);
+        if (sl.bp.win3) backward_tile<false, false, SEG, VB, true>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+        else backward_tile<false, false, SEG, VB, false>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+    }
+}
+
 template <int SEG, int VB>
 __global__ void __launch_bounds__(kBwdTile * kBwdTile, 4) k_backward_batch(const BatchArgs a)
 {
@@ -1056,12 +1531,7 @@ __global__ void __launch_bounds__(kBwdTile * kBwdTile, 4) k_backward_batch(const
         const int tile = (int)(item - a.prefix[i]);
         const bool fan = sl.bp.g.fan != 0;
         if (sl.tiled) {
-            if (fan)
-                backward_tile<true, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
-                                                    *reinterpret_cast<TiledSmem<true, SEG, VB> *>(raw));
-            else
-                backward_tile<false, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
-                                                     *reinterpret_cast<TiledSmem<false, SEG, VB> *>(raw));
+            batch_tile<SEG, VB>(sl, tile, raw);
         } else {
             if (fan) backward_tile_direct<true>(sl.bp, tile, sl.bsino, sl.bimg);
             else backward_tile_direct<false>(sl.bp, tile, sl.bsino, sl.bimg);
@@ -1123,12 +1593,7 @@ k_backward_stream(const BatchArgs a, const volatile int *__restrict__ ready,
         const int tile = (int)(item - a.prefix[i]);
         const bool fan = sl.bp.g.fan != 0;
         if (sl.tiled) {
-            if (fan)
-                backward_tile<true, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
-                                                    *reinterpret_cast<TiledSmem<true, SEG, VB> *>(raw));
-            else
-                backward_tile<false, false, SEG, VB>(sl.bp, tile, sl.bsino, sl.bimg,
-                                                     *reinterpret_cast<TiledSmem<false, SEG, VB> *>(raw));
+            batch_tile<SEG, VB>(sl, tile, raw);
         } else {
             if (fan) backward_tile_direct<true>(sl.bp, tile, sl.bsino, sl.bimg);
             else backward_tile_direct<false>(sl.bp, tile, sl.bsino, sl.bimg);

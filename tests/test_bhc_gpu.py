@@ -84,10 +84,18 @@ def test_fused_forward_and_adjoint_match_fp64_oracle_at_the_1024_configuration()
     """The polychromatic model's own configuration: fan 1024^2, 720 views over
     [0, 2 pi), 1024 detectors, source 2048 px from the isocentre, J = 20,
     two-material phantom, Poisson counts at I0 = 1e5 of the FP64 oracle's
-    intensity.  f, df/dx and df/dIe against the FP64 oracle (the FP64
-    projector restatement and oracle/bhc_oracle.py, bhc/poissLAlpha.m:1-19 and
-    bhc/poissLI.m:1-27): f within 1e-6 relative, both gradients within 1e-5
-    relative L2."""
+    intensity, against the FP64 oracle (the FP64 projector restatement and
+    oracle/bhc_oracle.py; bhc/poissLAlpha.m:1-19, bhc/poissLI.m:1-27).
+
+    f within 1e-6 and df/dx within 1e-5 relative L2.  df/dIe_j sums
+    b_j(s_i) (1 - m_i / BL_i) over 7.4e5 rays near the likelihood's optimum,
+    where the terms nearly cancel: a projection bias of 3e-8 (half a float32
+    unit) shared by all rays moves it by 6e-5 relative (the oracle's own
+    sensitivity, |sum_i |b_ij| |dBL/ds| s_i / BL_i| / |df/dIe|, is about
+    1900).  So df/dIe is checked twice: the FP64 epilogue on the GPU's own
+    float32 projections must agree with the oracle's epilogue on the same
+    projections to 1e-9, and against the all-FP64 oracle the error must stay
+    below what a common projection bias of 1e-7 would cause."""
     g = ct.Geometry(1024, 1024, 720, 720, 1.0, 1.0, 2048.0)
     x, k, Ie, m, Ts = problem(g, J=20, seed=4)
     pr = ct.Projector(g)
@@ -98,12 +106,26 @@ def test_fused_forward_and_adjoint_match_fp64_oracle_at_the_1024_configuration()
     dm = torch.from_numpy(m32).cuda()
     f = model.forward(dx, dI, dm).item()
     gx, gI = model.backward()
+    gI = gI.cpu().numpy()
+    mo = m32.astype(np.float64).ravel()
     fo, gxo, gIo = oracle_eval(g, x, k, Ie, m32.astype(np.float64), Ts)
-    ef, ex, eI = abs(f - fo) / abs(fo), rel(gx.cpu().numpy(), gxo), rel(gI.cpu().numpy(), gIo)
-    print("bhc fan 1024^2 / 720 views: f rel %.2e, grad_x rel %.2e, grad_Ie rel %.2e" % (ef, ex, eI))
+    ef, ex, eI = abs(f - fo) / abs(fo), rel(gx.cpu().numpy(), gxo), rel(gI, gIo)
+    # the oracle's epilogue on the GPU's own float32 projections
+    s_gpu = Ts * pr.forward(dx).double().cpu().numpy().ravel()
+    Bm, D, _ = BO.b1_basis(k, s_gpu)
+    BL = Bm @ Ie
+    eI_same = rel(gI, Bm.T @ (1 - mo / BL))
+    # sensitivity of df/dIe to a relative projection bias shared by all rays
+    s_o = Ts * oracle.forward(g, x.astype(np.float64)).ravel()
+    Bo, Do, _ = BO.b1_basis(k, s_o)
+    BLo = Bo @ Ie
+    amp = np.linalg.norm(np.abs(Bo.T) @ (np.abs(Do @ Ie) / BLo * s_o)) / np.linalg.norm(gIo)
+    print("bhc fan 1024^2 / 720 views: f rel %.2e, grad_x rel %.2e, grad_Ie rel %.2e (same projections "
+          "%.2e; sensitivity %.0f: equivalent projection bias %.1e)" % (ef, ex, eI, eI_same, amp, eI / amp))
     assert ef <= 1e-6
     assert ex < 1e-5
-    assert eI < 1e-5
+    assert eI_same < 1e-9
+    assert eI < 1e-7 * amp
 
 
 def test_fused_equals_unfused_and_recompute_equals_store():

@@ -51,3 +51,24 @@ def test_larger_case_against_oracle_and_adjoint():
     # A/bw and A^T/bw are transposes of each other
     err = abs(fx @ y - x @ by) / (np.linalg.norm(fx) * np.linalg.norm(y))
     assert err < 1e-12
+
+
+def test_forward_repeats_bit_for_bit_and_ignores_the_mask_order():
+    """The forward gathers per (angle, detector) without atomics: two runs give
+    identical bits, and listing the mask in another order (with x permuted the
+    same way) gives identical bits too, since the pixels are visited in image
+    order."""
+    rng = np.random.default_rng(8)
+    n, W, npv = 200, 287, 90
+    conf = dict(bw=1.0, nc=n, nr=n, prjWidth=W, theta=np.arange(npv) * 2.0 + 0.25)
+    yy, xx = np.mgrid[:n, :n]
+    disc = ((xx - n / 2) ** 2 + (yy - n / 2) ** 2) <= (0.47 * n) ** 2
+    mask = np.flatnonzero(disc.ravel(order="F")).astype(np.float64)
+    x = rng.standard_normal(mask.size)
+    a = mex.mParPrj(x, mask, conf, "forward")
+    b = mex.mParPrj(x, mask, conf, "forward")
+    assert np.array_equal(a, b)
+    perm = rng.permutation(mask.size)
+    c = mex.mParPrj(x[perm], mask[perm], conf, "forward")
+    assert np.array_equal(a, c)
+    assert rel(a, oracle.par_forward(x, mask, conf)) < 1e-12
