@@ -1057,6 +1057,92 @@ struct TiledSmem {
     FootprintV pfs[VB];
 };
 
+// Staging of one batch of VB base views for tile (tx, ty) (every thread of the
+// block takes part; ends with a block barrier): A, the tile's detector span
+// and centre per view; B1, the footprint coefficients of the staged
+// detectors; B2, their mirrored sinogram samples.
+template <bool FAN, int SEG, int VB>
+__device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__restrict__ sino, int tx, int ty,
+                                            double xc, double yc, int i0, int nb, TiledSmem<FAN, SEG, VB> &sm)
+{
+    const Geo &g = p.g;
+    auto &ra = sm.ra;
+    auto &rb = sm.rb;
+    auto &seg = sm.seg;
+    auto &seg2 = sm.seg2;
+    auto &tv = sm.tv;
+    auto &pfs = sm.pfs;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, kWarps = blockDim.x >> 5;
+    const int pC = g.pC;
+    // A: per view, the tile's detector span and centre
+    if (threadIdx.x < nb) {
+        const int iv = threadIdx.x;
+        const BwdView &bv = p.view[i0 + iv];
+        const TileSpan sp = tile_span(g, bv, tx, ty);
+        TileView t;
+        t.cT = bv.cf;
+        t.sT = bv.sf;
+        t.uc = fma(xc, bv.c, yc * bv.s);
+        t.vc = fma(yc, bv.c, -xc * bv.s);
+        t.ucf = (float)t.uc;
+        t.qec = (float)(g.d - t.vc);
+        t.hw = 0.5f * (fabsf(bv.cf) + fabsf(bv.sf));
+        t.A = 0.5f * (bv.cf + bv.sf);
+        t.B = 0.5f * (bv.cf - bv.sf);
+        t.AB = t.A * t.B;
+        t.klo = sp.klo;
+        t.nseg = min(sp.nseg, SEG);   // the plan chose SEG above every span
+        tv[iv] = t;
+        if (!FAN) pfs[iv] = make_footprint_v(bv.cf, bv.sf);
+    }
+    __syncthreads();
+    // B1: ray coefficients of the staged detectors, a warp per view
+    for (int iv = warp; iv < nb; iv += kWarps) {
+        const TileView &t = tv[iv];
+        for (int kk = lane; kk < t.nseg; kk += 32) {
+            const DetEntry &de = p.det[t.klo + kk + pC];
+            if (FAN) {
+                const double D = fma(de.cB, t.uc - de.t, de.sB * t.vc);
+                const float cR = fmaf(de.cBf, t.cT, -de.sBf * t.sT);
+                const float sR = fmaf(de.sBf, t.cT, de.cBf * t.sT);
+                const FootprintV f = make_footprint_v(cR, sR);
+                ra[iv][kk] = make_float4((float)D * f.iw, de.cBf * f.iw, de.sBf * f.iw,
+                                         0.5f * g.beamWidthF * de.invbq * f.iw);
+                rb[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.hw, f.tb, f.c1, f.rho);
+            } else {
+                ra[iv][kk] = make_float4((float)(t.uc - de.t) * pfs[iv].iw, 0.0f, 0.0f, 0.0f);
+            }
+        }
+    }
+    // B2: the mirrored sinogram samples, a warp per view, a lane per
+    // detector (each load instruction reads one sinogram row contiguously)
+    for (int iv = warp; iv < nb; iv += kWarps) {
+        const TileView &t = tv[iv];
+        const BwdView &bv = p.view[i0 + iv];
+        for (int kk = lane; kk < t.nseg; kk += 32) {
+            const int dt = t.klo + kk;
+            float v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int row = bv.row[j];
+                v[j] = row >= 0 ? __ldg(sino + row + pC + (j < 4 ? dt : -dt)) : 0.0f;
+            }
+            seg[iv][0][kk] = make_float4(v[0], v[1], v[2], v[3]);
+            seg[iv][1][kk] = make_float4(v[4], v[5], v[6], v[7]);
+            if (!FAN) {   // the point-reflected detectors of the opposite view
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int row2 = bv.row2[j];
+                    v[j] = row2 >= 0 ? __ldg(sino + row2 + pC - (j < 4 ? dt : -dt)) : 0.0f;
+                }
+                seg2[FAN ? 0 : iv][0][FAN ? 0 : kk] = make_float4(v[0], v[1], v[2], v[3]);
+                seg2[FAN ? 0 : iv][1][FAN ? 0 : kk] = make_float4(v[4], v[5], v[6], v[7]);
+            }
+        }
+    }
+    __syncthreads();
+}
+
 // One tile of the staged backprojection (all threads of the block take part).
 // WIN3: every pixel shadow of the plan is narrower than 1.9 detectors (the
 // plan's bound), so the detectors a pixel reaches in a view always lie within
@@ -1107,73 +1193,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
 
     for (int i0 = 0; i0 < p.nv; i0 += VB) {
         const int nb = min(VB, p.nv - i0);
-        // A: per view, the tile's detector span and centre
-        if (threadIdx.x < nb) {
-            const int iv = threadIdx.x;
-            const BwdView &bv = p.view[i0 + iv];
-            const TileSpan sp = tile_span(g, bv, tx, ty);
-            TileView t;
-            t.cT = bv.cf;
-            t.sT = bv.sf;
-            t.uc = fma(xc, bv.c, yc * bv.s);
-            t.vc = fma(yc, bv.c, -xc * bv.s);
-            t.ucf = (float)t.uc;
-            t.qec = (float)(g.d - t.vc);
-            t.hw = 0.5f * (fabsf(bv.cf) + fabsf(bv.sf));
-            t.A = 0.5f * (bv.cf + bv.sf);
-            t.B = 0.5f * (bv.cf - bv.sf);
-            t.AB = t.A * t.B;
-            t.klo = sp.klo;
-            t.nseg = min(sp.nseg, SEG);   // the plan chose SEG above every span
-            tv[iv] = t;
-            if (!FAN) pfs[iv] = make_footprint_v(bv.cf, bv.sf);
-        }
-        __syncthreads();
-        // B1: ray coefficients of the staged detectors, a warp per view
-        for (int iv = warp; iv < nb; iv += kWarps) {
-            const TileView &t = tv[iv];
-            for (int kk = lane; kk < t.nseg; kk += 32) {
-                const DetEntry &de = p.det[t.klo + kk + pC];
-                if (FAN) {
-                    const double D = fma(de.cB, t.uc - de.t, de.sB * t.vc);
-                    const float cR = fmaf(de.cBf, t.cT, -de.sBf * t.sT);
-                    const float sR = fmaf(de.sBf, t.cT, de.cBf * t.sT);
-                    const FootprintV f = make_footprint_v(cR, sR);
-                    ra[iv][kk] = make_float4((float)D * f.iw, de.cBf * f.iw, de.sBf * f.iw,
-                                             0.5f * g.beamWidthF * de.invbq * f.iw);
-                    rb[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.hw, f.tb, f.c1, f.rho);
-                } else {
-                    ra[iv][kk] = make_float4((float)(t.uc - de.t) * pfs[iv].iw, 0.0f, 0.0f, 0.0f);
-                }
-            }
-        }
-        // B2: the mirrored sinogram samples, a warp per view, a lane per
-        // detector (each load instruction reads one sinogram row contiguously)
-        for (int iv = warp; iv < nb; iv += kWarps) {
-            const TileView &t = tv[iv];
-            const BwdView &bv = p.view[i0 + iv];
-            for (int kk = lane; kk < t.nseg; kk += 32) {
-                const int dt = t.klo + kk;
-                float v[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int row = bv.row[j];
-                    v[j] = row >= 0 ? __ldg(sino + row + pC + (j < 4 ? dt : -dt)) : 0.0f;
-                }
-                seg[iv][0][kk] = make_float4(v[0], v[1], v[2], v[3]);
-                seg[iv][1][kk] = make_float4(v[4], v[5], v[6], v[7]);
-                if (!FAN) {   // the point-reflected detectors of the opposite view
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) {
-                        const int row2 = bv.row2[j];
-                        v[j] = row2 >= 0 ? __ldg(sino + row2 + pC - (j < 4 ? dt : -dt)) : 0.0f;
-                    }
-                    seg2[FAN ? 0 : iv][0][FAN ? 0 : kk] = make_float4(v[0], v[1], v[2], v[3]);
-                    seg2[FAN ? 0 : iv][1][FAN ? 0 : kk] = make_float4(v[4], v[5], v[6], v[7]);
-                }
-            }
-        }
-        __syncthreads();
+        stage_batch<FAN, SEG, VB>(p, sino, tx, ty, xc, yc, i0, nb, sm);
         // C: every pixel of the tile over the batch
         if (valid) {
             for (int iv = 0; iv < nb; ++iv) {
@@ -1314,6 +1334,134 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     if (valid) write_octant(p, img, x, y, nimg, S);
 }
 
+#if CTPRJ_BWD_PAIR
+// ------------------------------------- backward, two pixels per thread
+//
+// Build-time variant (CTPRJ_BWD_PAIR=1) of the fan-beam window kernel: a
+// thread owns two horizontally adjacent pixels of the tile (128 threads per
+// 16 x 16 tile), and for each view reads the staged detectors of the union of
+// their two windows once: three to five detectors for two pixels instead of
+// six.  Each pixel takes a weight for every detector of the union; those
+// outside its own window lie beyond its shadow and add exactly zero, so the
+// sums equal the one-pixel kernel's.
+template <bool FBP, int SEG, int VB>
+__global__ void __launch_bounds__(kBwdTile * kBwdTile / 2, 6)
+k_backward_pair(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
+{
+    __shared__ TiledSmem<true, SEG, VB> sm;
+    const Geo &g = p.g;
+    const int tile = blockIdx.x;
+    if (p.zero_axes && tile == 0)
+        for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
+            img[i] = 0.0f;
+            img[(size_t)i * g.n] = 0.0f;
+        }
+    int tx, ty;
+    decode_tile(tile, tx, ty);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // a warp takes 8 x 8 pixels: lane (2 (lane % 4), lane / 4) and its right
+    // neighbour.  Eight lanes of a quarter-warp then span 8 x 2 pixels, whose
+    // windows fall in consecutive staged detectors (16 x 1 would spread them
+    // over twice as many entries and double the shared-memory wavefronts)
+    const int x1 = tx * kBwdTile + ((warp & 1) << 3) + ((lane & 3) << 1), x2 = x1 + 1;
+    const int y = ty * kBwdTile + ((warp >> 1) << 3) + (lane >> 2);
+    const bool valid1 = x1 <= g.half && y <= x1, valid2 = x2 <= g.half && y <= x2;
+    const double xc = tx * kBwdTile + 0.5 * (kBwdTile - 1), yc = ty * kBwdTile + 0.5 * (kBwdTile - 1);
+    const float dx1 = (float)(x1 - xc), dx2 = (float)(x2 - xc), dy = (float)(y - yc);
+    const float dFs = (float)((double)g.dF / g.dSize);
+    float S1[8], S2[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) S1[j] = S2[j] = 0.0f;
+#if CTPRJ_BWD_PAIR == 2
+    unsigned long long A1[4] = {0ull, 0ull, 0ull, 0ull}, A2[4] = {0ull, 0ull, 0ull, 0ull};
+#endif
+
+    for (int i0 = 0; i0 < p.nv; i0 += VB) {
+        const int nb = min(VB, p.nv - i0);
+        stage_batch<true, SEG, VB>(p, sino, tx, ty, xc, yc, i0, nb, sm);
+        for (int iv = 0; iv < nb; ++iv) {
+            const TileView &t = sm.tv[iv];
+            const float du1 = fmaf(dx1, t.cT, dy * t.sT), du2 = fmaf(dx2, t.cT, dy * t.sT);
+            const float dv1 = fmaf(dy, t.cT, -dx1 * t.sT), dv2 = fmaf(dy, t.cT, -dx2 * t.sT);
+            const float qe1 = t.qec - dv1, qe2 = t.qec - dv2;
+            const float tc1 = __fdividef(dFs * (t.ucf + du1), qe1);
+            const float tc2 = __fdividef(dFs * (t.ucf + du2), qe2);
+            // each pixel's window (staged units, unclipped) and their union, as
+            // wide as the widest of the warp; a detector of the union outside
+            // the staged span [0, nseg) lies beyond the tile's reach or the
+            // detector's edge and is skipped
+            const int k1 = __float2int_rn(tc1) - 1 - t.klo, k2 = __float2int_rn(tc2) - 1 - t.klo;
+            const int un = __reduce_max_sync(0xffffffffu, max(k1, k2) - min(k1, k2) + 3);
+            const int kb = min(k1, k2);
+            const float fbpw1 = FBP ? __fdividef(g.dF, qe1) * __fdividef(g.dF, qe1) : 1.0f;
+            const float fbpw2 = FBP ? __fdividef(g.dF, qe2) * __fdividef(g.dF, qe2) : 1.0f;
+            auto slot = [&](const int kk) {
+                if ((unsigned)kk >= (unsigned)t.nseg) return;
+                const float4 a = sm.ra[iv][kk];
+                const float4 b = sm.rb[iv][kk];
+                const FootprintV f = {b.x, b.y, b.z, b.w, 0.0f};
+                float w1 = footprint_weight_v(fmaf(a.y, du1, fmaf(a.z, dv1, a.x)), qe1 * a.w, f);
+                float w2 = footprint_weight_v(fmaf(a.y, du2, fmaf(a.z, dv2, a.x)), qe2 * a.w, f);
+                if (FBP) {
+                    w1 *= fbpw1;
+                    w2 *= fbpw2;
+                }
+#if CTPRJ_BWD_PAIR == 2
+                // packed: {S[2i], S[2i+1]} += {w, w} {p[2i], p[2i+1]}, one
+                // fma.rn.f32x2 for two sums (each lane rounds as fmaf)
+                const ulonglong2 q0 = *reinterpret_cast<const ulonglong2 *>(&sm.seg[iv][0][kk]);
+                const ulonglong2 q1 = *reinterpret_cast<const ulonglong2 *>(&sm.seg[iv][1][kk]);
+                unsigned long long ww1, ww2;
+                asm("mov.b64 %0, {%1, %1};" : "=l"(ww1) : "f"(w1));
+                asm("mov.b64 %0, {%1, %1};" : "=l"(ww2) : "f"(w2));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A1[0]) : "l"(ww1), "l"(q0.x));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A1[1]) : "l"(ww1), "l"(q0.y));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A1[2]) : "l"(ww1), "l"(q1.x));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A1[3]) : "l"(ww1), "l"(q1.y));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A2[0]) : "l"(ww2), "l"(q0.x));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A2[1]) : "l"(ww2), "l"(q0.y));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A2[2]) : "l"(ww2), "l"(q1.x));
+                asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(A2[3]) : "l"(ww2), "l"(q1.y));
+#else
+                const float4 p0 = sm.seg[iv][0][kk], p1 = sm.seg[iv][1][kk];
+                S1[0] = fmaf(w1, p0.x, S1[0]);
+                S1[1] = fmaf(w1, p0.y, S1[1]);
+                S1[2] = fmaf(w1, p0.z, S1[2]);
+                S1[3] = fmaf(w1, p0.w, S1[3]);
+                S1[4] = fmaf(w1, p1.x, S1[4]);
+                S1[5] = fmaf(w1, p1.y, S1[5]);
+                S1[6] = fmaf(w1, p1.z, S1[6]);
+                S1[7] = fmaf(w1, p1.w, S1[7]);
+                S2[0] = fmaf(w2, p0.x, S2[0]);
+                S2[1] = fmaf(w2, p0.y, S2[1]);
+                S2[2] = fmaf(w2, p0.z, S2[2]);
+                S2[3] = fmaf(w2, p0.w, S2[3]);
+                S2[4] = fmaf(w2, p1.x, S2[4]);
+                S2[5] = fmaf(w2, p1.y, S2[5]);
+                S2[6] = fmaf(w2, p1.z, S2[6]);
+                S2[7] = fmaf(w2, p1.w, S2[7]);
+#endif
+            };
+            slot(kb);
+            slot(kb + 1);
+            slot(kb + 2);
+            if (un > 3) slot(kb + 3);
+            if (un > 4) slot(kb + 4);
+        }
+        __syncthreads();
+    }
+#if CTPRJ_BWD_PAIR == 2
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(S1[2 * j]), "=f"(S1[2 * j + 1]) : "l"(A1[j]));
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(S2[2 * j]), "=f"(S2[2 * j + 1]) : "l"(A2[j]));
+    }
+#endif
+    if (valid1) write_octant(p, img, x1, y, (y == 0 || y == x1) ? 4 : 8, S1);
+    if (valid2) write_octant(p, img, x2, y, (y == 0 || y == x2) ? 4 : 8, S2);
+}
+#endif
+
 template <bool FAN, bool FBP, int SEG, int VB, bool WIN3>
 __global__ void __launch_bounds__(kBwdTile * kBwdTile, CTPRJ_BWD_MINBLOCKS)
 k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
@@ -1426,6 +1574,17 @@ int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp
             if (fan) k_backward<true, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
             else k_backward<false, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
         }
+#if CTPRJ_BWD_PAIR
+    } else if (fan && p.win3) {
+        const dim3 pblock(kBwdTile * kBwdTile / 2);
+        if (pl->bwd_seg <= 32) {
+            if (fbp) k_backward_pair<true, 32, 16><<<grid, pblock, 0, s>>>(p, sino, img);
+            else k_backward_pair<false, 32, 16><<<grid, pblock, 0, s>>>(p, sino, img);
+        } else {
+            if (fbp) k_backward_pair<true, 64, 8><<<grid, pblock, 0, s>>>(p, sino, img);
+            else k_backward_pair<false, 64, 8><<<grid, pblock, 0, s>>>(p, sino, img);
+        }
+#endif
     } else if (pl->bwd_seg <= 32) {
         if (p.win3) launch_tiled<32, 16, true>(p, fan, fbp, grid, block, sino, img, s);
         else launch_tiled<32, 16, false>(p, fan, fbp, grid, block, sino, img, s);
