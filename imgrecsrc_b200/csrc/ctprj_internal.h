@@ -85,7 +85,7 @@ struct BwdParams {
     int zero_axes;            // even n: row 0 and column 0 written as zero
     float scale;              // output scale: FBP PI_f/np/dSize^2, BHC gradient Ts, else 1
     int fast_shadow;          // fan: pixel shadows from the first-order expansion (staged kernel)
-    int win3;                 // staged kernel: three detectors per pixel and view hold every shadow
+    int win;                  // staged kernel: 3 detectors per pixel and view hold every shadow; 0: range
     const BwdView *view;
     const DetEntry *det;
 };

@@ -395,6 +395,75 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
                 S[7] = fmaf(w, dm, S[7]);
             }
         };
+#if CTPRJ_FWD_PIPE
+        // Build-time variant (CTPRJ_FWD_PIPE=1): the window march software-
+        // pipelined two rows deep, the next row's gathers issued before this
+        // row's footprints (rows ya, ya - 1, ..., yb; q is row ya's quad row
+        // and moves by dq per row).  Same sums as march_win.
+        auto march_pipe = [&](const int ya, const int yb, const float4 *q, const int dq, auto neg, auto wn) {
+            constexpr bool NEG = decltype(neg)::value;
+            constexpr int WN = decltype(wn)::value;
+            struct Row {
+                float4 pp[WN], pm[WN];
+                int xs;
+                bool on;
+            };
+            auto fetch = [&](const int y, const float4 *__restrict__ qq, Row &R) {
+                const float xc = fmaf(-(float)y, Scf, Acf);
+                R.on = !(xc < -(float)half - 2.0f || xc > (float)half + 2.0f);
+                int xs = (WN == 3 ? __float2int_rn(xc) : __float2int_rd(xc)) - 1;
+                xs = min(max(xs, -half), half - (WN - 1));
+                R.xs = xs;
+#pragma unroll
+                for (int j = 0; j < WN; ++j) {
+                    R.pp[j] = __ldg(qq + xs + j);
+                    R.pm[j] = __ldg(qq - xs - j);
+                }
+            };
+            auto sum = [&](const int y, const Row &R) {
+                if (!R.on) return;
+                const float yf = (float)y;
+                const float r0 = (float)fma((double)R.xs, cR, fma((double)y, sR, -off)) * fp.iw;
+                const float hb0 = (FAN ? 0.5f * fmaf(fmaf((float)R.xs, sTf, -yf * cTf), kbw, bwc)
+                                       : 0.5f * g.beamWidthF) * fp.iw;
+#pragma unroll
+                for (int j = 0; j < WN; ++j) {
+                    const float D = fmaf((float)j, cRw, r0);
+                    const float H = FAN ? fmaf((float)j, dhbw, hb0) : hb0;
+                    const float w = footprint_weight_v(D, H, fp);
+                    const float4 pp = R.pp[j], pm = R.pm[j];
+                    S[0] = fmaf(w, NEG ? pp.y : pp.x, S[0]);
+                    S[6] = fmaf(w, NEG ? pm.y : pm.x, S[6]);
+                    S[4] = fmaf(w, NEG ? pp.x : pp.y, S[4]);
+                    S[2] = fmaf(w, NEG ? pm.x : pm.y, S[2]);
+                    S[5] = fmaf(w, NEG ? pp.w : pp.z, S[5]);
+                    S[3] = fmaf(w, NEG ? pm.w : pm.z, S[3]);
+                    S[1] = fmaf(w, NEG ? pp.z : pp.w, S[1]);
+                    S[7] = fmaf(w, NEG ? pm.z : pm.w, S[7]);
+                }
+            };
+            Row A, B;
+            fetch(ya, q, A);
+            int y = ya;
+            for (; y - 1 >= yb; y -= 2, q += 2 * dq) {
+                fetch(y - 1, q + dq, B);
+                sum(y, A);
+                if (y - 2 >= yb) fetch(y - 2, q + 2 * dq, A);
+                sum(y - 1, B);
+            }
+            if (y == yb) sum(y, A);
+        };
+        if (wcode == 3 || wcode == 4) {
+            const float4 *qp = quad + (size_t)half * QW + half, *qn = quad + (size_t)QW + half;
+            if (wcode == 3) {
+                march_pipe(half, 0, qp, -QW, std::false_type{}, std::integral_constant<int, 3>{});
+                march_pipe(-1, -half, qn, QW, std::true_type{}, std::integral_constant<int, 3>{});
+            } else {
+                march_pipe(half, 0, qp, -QW, std::false_type{}, std::integral_constant<int, 4>{});
+                march_pipe(-1, -half, qn, QW, std::true_type{}, std::integral_constant<int, 4>{});
+            }
+        } else
+#endif
         {
             const float4 *q = quad + (size_t)half * QW + half;   // row |y| = half, x = 0
             if (wcode == 3) {
@@ -1144,15 +1213,17 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
 }
 
 // One tile of the staged backprojection (all threads of the block take part).
-// WIN3: every pixel shadow of the plan is narrower than 1.9 detectors (the
+// WIN = 3: every pixel shadow of the plan is narrower than 1.9 detectors (the
 // plan's bound), so the detectors a pixel reaches in a view always lie within
-// the three centred on the projection of its centre: those three are summed
-// straight, without the per-pixel shadow range.  A detector of the three that
-// the reference's range rule (prj/cpuPrj.c:218-244) leaves out lies beyond the
-// pixel's footprint and adds a weight of exactly zero, except within ~1e-4
-// detector of a shadow edge, where the footprint and the exact corner shadow
-// differ and the weight is below 1e-7.
-template <bool FAN, bool FBP, int SEG, int VB, bool WIN3>
+// the three centred on the projection of its centre, tc; WIN = 4: narrower
+// than 2.85, and they lie within the four from floor(tc) - 1.  Those detectors
+// are summed straight, without the per-pixel shadow range (WIN = 0: the
+// range).  A detector of the window that the reference's range rule
+// (prj/cpuPrj.c:218-244) leaves out lies beyond the pixel's footprint and adds
+// a weight of exactly zero, except within ~1e-4 detector of a shadow edge,
+// where the footprint and the exact corner shadow differ and the weight is
+// below 1e-7.
+template <bool FAN, bool FBP, int SEG, int VB, int WIN>
 __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                                               const float *__restrict__ sino,
                                               float *__restrict__ img,
@@ -1201,17 +1272,18 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                 const float du = fmaf(dx, t.cT, dy * t.sT);
                 const float dv = fmaf(dy, t.cT, -dx * t.sT);
                 const float u = t.ucf + du;
-                if (WIN3 && t.nseg >= 3) {   // t.nseg is the same for the whole block
+                if (WIN > 0 && t.nseg >= WIN) {   // t.nseg is the same for the whole block
                     const float qe = FAN ? t.qec - dv : 0.0f;
                     // the detector under the pixel centre, in staged units
                     const float tc = FAN ? __fdividef(dFs * u, qe) : u * invdS;
-                    const int k0 = min(max(__float2int_rn(tc) - 1 - t.klo, 0), t.nseg - 3);
+                    const int ks = WIN == 3 ? __float2int_rn(tc) : __float2int_rd(tc);
+                    const int k0 = min(max(ks - 1 - t.klo, 0), t.nseg - WIN);
                     const float fbpw = FBP ? __fdividef(g.dF, qe) * __fdividef(g.dF, qe) : 1.0f;
                     const FootprintV fpar = FAN ? FootprintV{} : pfs[iv];
                     const float duw = FAN ? 0.0f : du * fpar.iw, Hpar = FAN ? 0.0f : hbpar * fpar.iw;
-                    float w[3];
+                    float w[WIN > 0 ? WIN : 1];
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
+                    for (int q = 0; q < WIN; ++q) {
                         const float4 a = ra[iv][k0 + q];
                         if (FAN) {
                             const float D = fmaf(a.y, du, fmaf(a.z, dv, a.x));
@@ -1224,7 +1296,7 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                         }
                     }
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
+                    for (int q = 0; q < WIN; ++q) {
                         const float4 p0 = seg[iv][0][k0 + q], p1 = seg[iv][1][k0 + q];
                         S[0] = fmaf(w[q], p0.x, S[0]);
                         S[1] = fmaf(w[q], p0.y, S[1]);
@@ -1462,12 +1534,12 @@ k_backward_pair(const BwdParams p, const float *__restrict__ sino, float *__rest
 }
 #endif
 
-template <bool FAN, bool FBP, int SEG, int VB, bool WIN3>
+template <bool FAN, bool FBP, int SEG, int VB, int WIN>
 __global__ void __launch_bounds__(kBwdTile * kBwdTile, CTPRJ_BWD_MINBLOCKS)
 k_backward_tiled(const BwdParams p, const float *__restrict__ sino, float *__restrict__ img)
 {
     __shared__ TiledSmem<FAN, SEG, VB> sm;
-    backward_tile<FAN, FBP, SEG, VB, WIN3>(p, blockIdx.x, sino, img, sm);
+    backward_tile<FAN, FBP, SEG, VB, WIN>(p, blockIdx.x, sino, img, sm);
 }
 
 // upper bound of a pixel's shadow width in detectors, or 0 where none holds
@@ -1515,12 +1587,15 @@ static BwdParams bwd_params(const ctprj_plan *pl, int fbp, float scale)
     // pixel nearest the source (R: the image corner's distance from the
     // isocentre) and the detector's obliquity adds 1 + tan^2 of the fan
     // angle, tan <= R / (d - R).  Below 1.9 detectors the three detectors
-    // centred on a pixel's projection hold its whole shadow.  A beam wider than
-    // the detector pitch (effectiveRate > 1) also reaches detectors outside the
-    // shadow, which the reference's range rule leaves out: such plans keep the
-    // per-pixel range.
+    // centred on a pixel's projection hold its whole shadow.  (Below 2.85 the
+    // four from floor(tc) - 1 would, but at the 1024^2 fan configuration, the
+    // one such plan measured, four straight detectors ran slower than the
+    // range: 1.82 against 1.66 ms per polychromatic gradient iteration.)  A
+    // beam wider than the detector pitch (effectiveRate > 1) also reaches
+    // detectors outside the shadow, which the reference's range rule leaves
+    // out: such plans keep the per-pixel range.
     const double width = shadow_width_bound(pl->g);
-    p.win3 = width > 0.0 && width <= 1.9 && pl->g.effRate <= 1.0f;
+    p.win = width > 0.0 && width <= 1.9 && pl->g.effRate <= 1.0f ? 3 : 0;
     return p;
 }
 
@@ -1543,17 +1618,25 @@ int backward_max_span(const ctprj_plan *pl, int *max_span)
     return st;
 }
 
-template <int SEG, int VB, bool WIN3>
+template <int SEG, int VB, int WIN>
+static void launch_tiled_win(const BwdParams &p, bool fan, int fbp, dim3 grid, dim3 block,
+                             const float *sino, float *img, cudaStream_t s)
+{
+    if (fan) {
+        if (fbp) k_backward_tiled<true, true, SEG, VB, WIN><<<grid, block, 0, s>>>(p, sino, img);
+        else k_backward_tiled<true, false, SEG, VB, WIN><<<grid, block, 0, s>>>(p, sino, img);
+    } else {
+        if (fbp) k_backward_tiled<false, true, SEG, VB, WIN><<<grid, block, 0, s>>>(p, sino, img);
+        else k_backward_tiled<false, false, SEG, VB, WIN><<<grid, block, 0, s>>>(p, sino, img);
+    }
+}
+
+template <int SEG, int VB>
 static void launch_tiled(const BwdParams &p, bool fan, int fbp, dim3 grid, dim3 block,
                          const float *sino, float *img, cudaStream_t s)
 {
-    if (fan) {
-        if (fbp) k_backward_tiled<true, true, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
-        else k_backward_tiled<true, false, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
-    } else {
-        if (fbp) k_backward_tiled<false, true, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
-        else k_backward_tiled<false, false, SEG, VB, WIN3><<<grid, block, 0, s>>>(p, sino, img);
-    }
+    if (p.win == 3) launch_tiled_win<SEG, VB, 3>(p, fan, fbp, grid, block, sino, img, s);
+    else launch_tiled_win<SEG, VB, 0>(p, fan, fbp, grid, block, sino, img, s);
 }
 
 int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp,
@@ -1575,7 +1658,7 @@ int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp
             else k_backward<false, false, false><<<grid, block, 0, s>>>(p, sino, img, counter);
         }
 #if CTPRJ_BWD_PAIR
-    } else if (fan && p.win3) {
+    } else if (fan && p.win == 3) {
         const dim3 pblock(kBwdTile * kBwdTile / 2);
         if (pl->bwd_seg <= 32) {
             if (fbp) k_backward_pair<true, 32, 16><<<grid, pblock, 0, s>>>(p, sino, img);
@@ -1586,11 +1669,9 @@ int launch_backward(const ctprj_plan *pl, const float *sino, float *img, int fbp
         }
 #endif
     } else if (pl->bwd_seg <= 32) {
-        if (p.win3) launch_tiled<32, 16, true>(p, fan, fbp, grid, block, sino, img, s);
-        else launch_tiled<32, 16, false>(p, fan, fbp, grid, block, sino, img, s);
+        launch_tiled<32, 16>(p, fan, fbp, grid, block, sino, img, s);
     } else {
-        if (p.win3) launch_tiled<64, 8, true>(p, fan, fbp, grid, block, sino, img, s);
-        else launch_tiled<64, 8, false>(p, fan, fbp, grid, block, sino, img, s);
+        launch_tiled<64, 8>(p, fan, fbp, grid, block, sino, img, s);
     }
     return cuda_error(cudaGetLastError(), "backward launch");
 }
@@ -1668,12 +1749,12 @@ __device__ __forceinline__ void batch_tile(const BatchSlice &sl, int tile, unsig
 {
     if (sl.bp.g.fan) {
         auto &sm = *reinterpret_cast<TiledSmem<true, SEG, VB> *>(raw);
-        if (sl.bp.win3) backward_tile<true, false, SEG, VB, true>(sl.bp, tile, sl.bsino, sl.bimg, sm);
-        else backward_tile<true, false, SEG, VB, false>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+        if (sl.bp.win == 3) backward_tile<true, false, SEG, VB, 3>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+        else backward_tile<true, false, SEG, VB, 0>(sl.bp, tile, sl.bsino, sl.bimg, sm);
     } else {
         auto &sm = *reinterpret_cast<TiledSmem<false, SEG, VB> *>(raw);
-        if (sl.bp.win3) backward_tile<false, false, SEG, VB, true>(sl.bp, tile, sl.bsino, sl.bimg, sm);
-        else backward_tile<false, false, SEG, VB, false>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+        if (sl.bp.win == 3) backward_tile<false, false, SEG, VB, 3>(sl.bp, tile, sl.bsino, sl.bimg, sm);
+        else backward_tile<false, false, SEG, VB, 0>(sl.bp, tile, sl.bsino, sl.bimg, sm);
     }
 }
 
