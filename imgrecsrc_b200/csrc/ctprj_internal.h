@@ -73,6 +73,7 @@ struct FwdParams {
     Geo g;
     int nb, k0, nk;           // base views, first ray, rays per base view
     int zero_col0;            // even prjWidth: detector 0 written as zero
+    int sms;                  // multiprocessors of the plan's device
     const FwdView *view;
     const DetEntry *det;
     BhcArgs bhc;

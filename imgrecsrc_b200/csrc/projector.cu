@@ -544,12 +544,25 @@ k_forward(const FwdParams p, const float4 *__restrict__ quad, float *__restrict_
         tab = sm;
         Ie = sm + kMaxJ * kSplStride;
     }
-    const double fsum = forward_rays<FAN, MODE, kFwdViews>(p, blockIdx.x, blockIdx.y, quad, sino,
-                                                           counter, tab, Ie);
+    int bx = blockIdx.x, by = blockIdx.y;
+#if CTPRJ_FWD_REMAP
+    // Build-time variant: the block scheduler starts blocks i, i + S, i + 2S, ...
+    // (S = SM count) on one SM in its first wave, so hand them consecutive view
+    // groups of one ray group: their rays cross nearly the same quad-image
+    // lines and could share that SM's L1.  A bijection of the block indices.
+    {
+        const int S = p.sms, total = gridDim.x * gridDim.y, i = blockIdx.y * gridDim.x + blockIdx.x;
+        const int q = total / S, r = total % S, sl = i % S, k = i / S;
+        const int item = sl * q + min(sl, r) + k;
+        bx = item % gridDim.x;
+        by = item / gridDim.x;
+    }
+#endif
+    const double fsum = forward_rays<FAN, MODE, kFwdViews>(p, bx, by, quad, sino, counter, tab, Ie);
     if constexpr (MODE == kModeBhc) {
         __shared__ double red[kFwdThreads / 32];
         const double t = block_sum(fsum, red);
-        if (threadIdx.x == 0) p.bhc.part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+        if (threadIdx.x == 0) p.bhc.part[(size_t)by * gridDim.x + bx] = t;
     }
 }
 
@@ -810,6 +823,8 @@ k_forward_staged(const FwdParams p, const float4 *__restrict__ quad, float *__re
 static FwdParams fwd_params(const ctprj_plan *pl)
 {
     FwdParams p;
+    p.sms = 148;
+    cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, pl->device);
     p.g = pl->g;
     p.nb = pl->nb;
     p.k0 = pl->k0;
