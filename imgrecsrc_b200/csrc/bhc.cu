@@ -329,6 +329,7 @@ static BhcArgs bhc_args(ctprj_bhc *m, const double *d_Ie, const float *d_imea, i
     a.w_out = keep ? m->d_w : nullptr;
     a.part = m->d_part;
     a.noise = m->noise;
+    a.proj_out = nullptr;
     return a;
 }
 
@@ -347,6 +348,21 @@ extern "C" int ctprj_bhc_forward(ctprj_bhc *m, const float *d_x, const double *d
         return st;
     k_sum_columns<<<1, 256, 0, s>>>(m->d_part, nparts, 1, d_f);
     m->saved = save ? 1 : 0;
+    return cuda_error(cudaGetLastError(), "likelihood reduction");
+}
+
+int ctprj::bhc_forward_keep_projection(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *d_imea,
+                                       double *d_f, float *proj, cudaStream_t s)
+{
+    int st;
+    if ((st = ensure_parts(m, forward_blocks(m->plan)))) return st;
+    if ((st = launch_quad(d_x, m->plan->d_quad, m->plan->g.n, s))) return st;
+    BhcArgs a = bhc_args(m, d_Ie, d_imea, 1);
+    a.proj_out = proj;
+    int nparts = 0;
+    if ((st = launch_forward_bhc(m->plan, m->plan->d_quad, a, &nparts, s))) return st;
+    k_sum_columns<<<1, 256, 0, s>>>(m->d_part, nparts, 1, d_f);
+    m->saved = 1;
     return cuda_error(cudaGetLastError(), "likelihood reduction");
 }
 

@@ -825,11 +825,12 @@ extern "C" int ctprj_bhc_spectrum_step(ctprj_bhc *m, const float *d_imea, double
 namespace {
 
 // the likelihood at (x, Ie), fused or from the plain projection; the per-ray
-// state is saved (the spectrum step and the gradient read it)
+// state is saved (the spectrum step and the gradient read it) and the plain
+// projection A x is left in sino either way
 int likelihood(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *d_imea, double *d_f,
-               float *sino, cudaStream_t s)
+               bool unfused, float *sino, cudaStream_t s)
 {
-    if (!sino) return ctprj_bhc_forward(m, d_x, d_Ie, d_imea, d_f, 1, s);
+    if (!unfused) return bhc_forward_keep_projection(m, d_x, d_Ie, d_imea, d_f, sino, s);
     int st = ctprj_forward(m->plan, d_x, sino, s);
     if (st) return st;
     return ctprj_bhc_terms(m, sino, d_Ie, d_imea, d_f, 1, s);
@@ -866,11 +867,12 @@ double reduce_fetch(const double *part, int nblocks, double *d_out, cudaStream_t
 // reference's NPG then stops with "a negative step size") is taken by its
 // magnitude.
 int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *d_imea, int mode,
-                         LoopBufs &b, int pgb, double *t_out, cudaStream_t s, const unsigned char *pmask)
+                         LoopBufs &b, int pgb, double *t_out, cudaStream_t s, const unsigned char *pmask,
+                         bool unfused)
 {
     const long long npx = (long long)m->plan->g.n * m->plan->g.n;
     int st = 0;
-    if ((st = likelihood(m, d_x, d_Ie, d_imea, b.f, b.sino, s)) ||
+    if ((st = likelihood(m, d_x, d_Ie, d_imea, b.f, unfused, b.sino, s)) ||
         (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.gx, nullptr, s)))
         return st;
     if (pmask) k_mask_apply<<<pgb, 256, 0, s>>>(b.gx, pmask, npx);
@@ -891,7 +893,7 @@ int initial_inverse_step(ctprj_bhc *m, const float *d_x, const double *d_Ie, con
         const double scale = dn / sqrt(gg);   // delta = scale * g
         k_axpy<<<pgb, 256, 0, s>>>(d_x, b.gx, (float)(-scale), npx, b.xbar);
         if ((st = cuda_error(cudaGetLastError(), "BB step")) ||
-            (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, b.sino, s)) ||
+            (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, unfused, b.sino, s)) ||
             (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.xn, nullptr, s)))
             return st;
         if (pmask) k_mask_apply<<<pgb, 256, 0, s>>>(b.xn, pmask, npx);
@@ -985,8 +987,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         (reg && (st = cuda_error(cudaMalloc((void **)&b.v, sizeof(float) * npx), "loop buffers"))) ||
         (tv && (st = tvw.alloc(n, n, s))) ||
         (wv && (st = wws.alloc(n, n, s))) ||
-        (opts->unfused &&
-         (st = cuda_error(cudaMalloc((void **)&b.sino, sizeof(float) * nr), "loop buffers"))) ||
+        (st = cuda_error(cudaMalloc((void **)&b.sino, sizeof(float) * nr), "loop buffers")) ||
         (!opts->skip_spectrum && (st = ws.alloc(m->J, nr, spectrum_grid(dev), s)))) {
         tvw.release(s);
         wws.release(s);
@@ -1051,10 +1052,15 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         st = cuda_error(cudaMemcpyAsync(b.xprev, d_x, sizeof(float) * npx, cudaMemcpyDeviceToDevice, s), "loop start");
     cudaEventRecord(e0, s);
     if (!st && opts->init_step != CTPRJ_STEP_FIXED) {
-        st = initial_inverse_step(m, d_x, d_Ie, d_imea, opts->init_step, b, pgb, &t, s, opts->mask);
+        st = initial_inverse_step(m, d_x, d_Ie, d_imea, opts->init_step, b, pgb, &t, s, opts->mask,
+                                  opts->unfused != 0);
         evals += opts->init_step == CTPRJ_STEP_BB ? 2 : 1;
     }
     int done = 0;
+    // b.sino holds A x for the current x: PG's next extrapolated point is x
+    // itself, so its likelihood needs no new projection, only the terms at the
+    // current spectrum (the same sums: the projection is deterministic)
+    bool proj_at_x = false;
     for (int it = 0; it < opts->iterations && !st; ++it) {
         double nc = 0.0, obj = 0.0;
         bool moved = false, state_at_x = false;
@@ -1067,9 +1073,11 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
             k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 1, b.sum + 1);
             double f0 = 0.0, mom = 0.0;
             if ((st = cuda_error(cudaGetLastError(), "extrapolation")) ||
-                (st = likelihood(m, b.xbar, d_Ie, d_imea, b.f, b.sino, s)) ||
+                (st = (pg && proj_at_x) ? ctprj_bhc_terms(m, b.sino, d_Ie, d_imea, b.f, 1, s)
+                                        : likelihood(m, b.xbar, d_Ie, d_imea, b.f, opts->unfused != 0, b.sino, s)) ||
                 (st = ctprj_bhc_backward(m, nullptr, nullptr, nullptr, b.gx, nullptr, s)))
                 break;
+            proj_at_x = pg;   // xbar = x for PG
             if (pmask) k_mask_apply<<<pgb, 256, 0, s>>>(b.gx, pmask, npx);   // the masked gradient
             if ((st = cuda_error(cudaMemcpyAsync(&mom, b.sum + 1, sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
                 (st = fetch(&f0, b.f, 1, s)))
@@ -1104,10 +1112,11 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                 k_ie_sum<<<1, 256, 0, s>>>(b.part, pgb, 2, 2, b.sum);
                 double gd_dd[2];
                 if ((st = cuda_error(cudaGetLastError(), "density step")) ||
-                    (st = likelihood(m, b.xn, d_Ie, d_imea, b.f + 1, b.sino, s)) ||
+                    (st = likelihood(m, b.xn, d_Ie, d_imea, b.f + 1, opts->unfused != 0, b.sino, s)) ||
                     (st = cuda_error(cudaMemcpyAsync(gd_dd, b.sum, 2 * sizeof(double), cudaMemcpyDeviceToHost, s), "readback")) ||
                     (st = fetch(&nc, b.f + 1, 1, s)))
                     break;
+                proj_at_x = false;   // b.sino now holds A xn
                 ++evals;
                 if (nc - f0 <= gd_dd[0] + 0.5 * t * gd_dd[1]) {
                     if (p <= pre_steps && ppp < 18 && good) {
@@ -1164,6 +1173,7 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
                     dif_alpha = sqrt(dq[0]) / fmax(sqrt(dq[1]), 1e-10);
             }
             state_at_x = moved;   // the last likelihood evaluated (and saved) was at xn
+            proj_at_x = moved;
             cumu = (ppp == 1 && adaptive) ? cumu + 1 : 0;
             break;
         }
@@ -1173,7 +1183,8 @@ extern "C" int ctprj_bhc_reconstruct(ctprj_bhc *m, float *d_x, double *d_Ie, con
         if (!opts->skip_spectrum) {
             cudaEventRecord(es0, s);
             if (!state_at_x) {
-                if ((st = likelihood(m, d_x, d_Ie, d_imea, b.f, b.sino, s))) break;
+                if ((st = likelihood(m, d_x, d_Ie, d_imea, b.f, opts->unfused != 0, b.sino, s))) break;
+                proj_at_x = true;
                 ++evals;
             }
             double fs = 0.0;

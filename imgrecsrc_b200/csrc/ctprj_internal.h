@@ -65,6 +65,7 @@ struct BhcArgs {
                               // all rays with cancellation, which single precision would not survive
     double *part;             // per-block partial sums of the likelihood terms
     int noise;                // kNoisePoisson or kNoiseGaussian
+    float *proj_out;          // the plain projection of each entry (np * prjWidth); NULL: not kept
 };
 
 enum { kModePlain = 0, kModeCount = 1, kModeBhc = 2 };
@@ -272,6 +273,10 @@ int launch_forward(const ctprj_plan *p, const float4 *quad, float *sino,
 // per-block partials written to a.part
 int launch_forward_bhc(const ctprj_plan *p, const float4 *quad,
                        const BhcArgs &a, int *nparts, cudaStream_t s);
+// the fused likelihood of ctprj_bhc_forward (state saved) that also keeps the
+// plain projection A x in proj (bhc.cu)
+int bhc_forward_keep_projection(ctprj_bhc *m, const float *d_x, const double *d_Ie, const float *d_imea,
+                                double *d_f, float *proj, cudaStream_t s);
 int forward_blocks(const ctprj_plan *p);
 int backward_max_span(const ctprj_plan *p, int *max_span);
 FwdParams make_fwd_params(const ctprj_plan *p);

@@ -222,8 +222,12 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
     // detector 0 of an even-width sinogram: no ray, zero projection
     if (MODE != kModeCount && p.zero_col0 && bx == 0 && by == 0)
         for (int v = threadIdx.x; v < g.np; v += blockDim.x) {
-            if constexpr (MODE == kModeBhc) fsum += bhc_entry(p.bhc, tab, Ie, 0.0f, (size_t)v * g.W);
-            else sino[(size_t)v * g.W] = 0.0f;
+            if constexpr (MODE == kModeBhc) {
+                fsum += bhc_entry(p.bhc, tab, Ie, 0.0f, (size_t)v * g.W);
+                if (p.bhc.proj_out) p.bhc.proj_out[(size_t)v * g.W] = 0.0f;
+            } else {
+                sino[(size_t)v * g.W] = 0.0f;
+            }
         }
 
     // The window a warp marches with (below) is the widest any of its rays
@@ -523,7 +527,10 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
         }
         if constexpr (MODE == kModeBhc) {
 #pragma unroll 1
-            for (int e = 0; e < ne; ++e) fsum += bhc_entry(p.bhc, tab, Ie, eval[e], (size_t)eidx[e]);
+            for (int e = 0; e < ne; ++e) {
+                fsum += bhc_entry(p.bhc, tab, Ie, eval[e], (size_t)eidx[e]);
+                if (p.bhc.proj_out) p.bhc.proj_out[eidx[e]] = eval[e];
+            }
         }
         if (MODE == kModeCount && nz * entries) atomicAdd(counter, nz * entries);
     }
