@@ -295,6 +295,7 @@ def our_arm(args):
     prof = profiled_kernels().get("k_backward_tiled<fan>" if bwd_ms >= fwd_ms else "k_forward<fan>", {})
     traffic = prof.get("dram_bytes_per_launch")
     issue = issue_roof(prof, kname, kms, clk.get("sm_mhz"), nnz_b if bwd_ms >= fwd_ms else nnz_f)
+    shared = shared_roof(prof, kname, kms, clk.get("sm_mhz"))
 
     bhc_line = batch_line = extras_line = loop_line = None
     if args.legs == "all":
@@ -362,6 +363,8 @@ def our_arm(args):
         "clocks": clk,
     }
     line["roofline"]["issue"] = issue
+    if shared:
+        line["roofline"]["shared"] = shared
     if rank == 0 and world == 1 and not args.no_cpu:
         # the reference's cpuPrj.c on the headline workload itself: 1 warm-up
         # and 3 timed passes (about 25 s on a 16-core host)
@@ -392,6 +395,8 @@ def summary(line):
     out = {"fwd_ms": r(c["fwd_ms"]), "bwd_ms": r(c["bwd_ms"]), "gray_px_s": r(line["value"]),
            "e2e_gray_px_s": r(line["e2e"]["value"]),
            "issue_frac": r((line["roofline"].get("issue") or {}).get("frac"), 3)}
+    if line["roofline"].get("shared"):
+        out["shared_frac"] = r(line["roofline"]["shared"]["frac"], 3)
     if "cpu_baseline" in line:
         out["cpu_gray_px_s"] = r(line["cpu_baseline"]["value"])
     for key, b in (line.get("bhc") or {}).items():
@@ -738,6 +743,20 @@ def issue_roof(prof, kname, kms, sm_mhz, updates):
             "frac": inst / slots, "sm_mhz": sm_mhz,
             "thread_inst_per_update": 32.0 * inst / updates,
             "source": "profiles/projector_counters.json (ncu smsp__inst_executed.sum)"}
+
+
+def shared_roof(prof, kname, kms, sm_mhz):
+    """The shared-memory roof of the staged backprojection: its shared-memory
+    wavefronts per launch (ncu l1tex__data_pipe_lsu_wavefronts_mem_shared.sum)
+    over the wavefront slots of its CUDA-event duration at the sampled SM clock
+    (148 SMs x 1 wavefront per cycle)."""
+    wf = prof.get("shared_wavefronts_per_launch")
+    if not wf or not sm_mhz:
+        return None
+    slots = kms * 1e-3 * SMS * sm_mhz * 1e6
+    return {"kernel": kname, "wavefronts_per_launch": wf, "wavefront_slots_per_launch": slots,
+            "frac": wf / slots, "sm_mhz": sm_mhz,
+            "source": "profiles/projector_counters.json (ncu l1tex__data_pipe_lsu_wavefronts_mem_shared.sum)"}
 
 
 def relaunch(args, argv):

@@ -59,17 +59,20 @@ __device__ __forceinline__ float footprint_weight(float dist, float bw, const Fo
 //   G(u) = h w/2 (P^2 - R'^2) + h 2 b1 Q + h w/2,
 //   P = sat(b2/w + v),  R' = sat(b2/w - v),  Q = sat(1/2 + v w/(2 b1))
 // (P: the rising ramp, R' = 1 - the falling ramp, Q: the plateau), and the
-// constant cancels in the difference of the two beam edges.  Callers pass the
-// distance and the half beam width already multiplied by 1/w (folded into
-// their per-ray coefficients), so a weight costs 14 arithmetic instructions.
+// constant cancels in the difference of the two beam edges.  With
+// hi = max(|c|,|s|) and lo = min(|c|,|s|): h = 1/hi, w = lo, 2 b1 = hi - lo, so
+// the plateau's factor h 2 b1 = 1 - lo/hi = 1 - 2 (h w/2) and the difference
+// is hw (dX - 2 dQ) + dQ with hw = h w/2: a footprint is three numbers (hw,
+// b2/w, w/(2 b1)) besides the scale 1/w.  Callers pass the distance and the
+// half beam width already multiplied by 1/w (folded into their per-ray
+// coefficients), so a weight costs 14 arithmetic instructions.
 // A ramp width or shoulder width of zero (axis-aligned or diagonal rays) gets
 // a tiny floor: the huge ratios saturate and are multiplied by the zero width,
 // so no branch is needed.  The rounding of b2/w +- v is bounded by
 // b2 ulp(1) / w and is scaled back by h w/2: the absolute error stays below
 // ~1e-7 for any ramp width.
 struct FootprintV {
-    float hw;    // h w / 2
-    float tb;    // h 2 b1
+    float hw;    // h w / 2 (the plateau's factor h 2 b1 is 1 - 2 hw)
     float c1;    // b2 / w
     float rho;   // w / (2 b1)
     float iw;    // 1 / w: the caller's scale of distances and beam widths
@@ -85,7 +88,6 @@ __host__ __device__ __forceinline__ FootprintV make_footprint_v(float c, float s
     q.c1 = f.b2 * q.iw;
     q.rho = w / tb;
     q.hw = f.h * 0.5f * f.w;
-    q.tb = f.h * 2.0f * f.b1;
     return q;
 }
 
@@ -98,7 +100,8 @@ __device__ __forceinline__ float footprint_weight_v(float D, float H, const Foot
     const float P2 = __saturatef(q.c1 + v2), R2 = __saturatef(q.c1 - v2);
     const float Q1 = __saturatef(fmaf(v1, q.rho, 0.5f)), Q2 = __saturatef(fmaf(v2, q.rho, 0.5f));
     const float X1 = fmaf(P1, P1, -R1 * R1), X2 = fmaf(P2, P2, -R2 * R2);
-    return fmaf(q.hw, X1 - X2, q.tb * (Q1 - Q2));
+    const float dQ = Q1 - Q2;
+    return fmaf(q.hw, fmaf(-2.0f, dQ, X1 - X2), dQ);
 }
 
 }  // namespace ctprj
