@@ -1112,6 +1112,38 @@ __device__ __forceinline__ TileSpan tile_span(const Geo &g, const BwdView &bv, i
     return sp;
 }
 
+// The same span from a full warp: lane l takes corner l % 4, the four
+// corners' projections are reduced over aligned groups of four lanes (min and
+// max are exact, so every lane gets tile_span's result)
+__device__ __forceinline__ TileSpan tile_span_lanes(const Geo &g, const BwdView &bv, int tx, int ty, int lane)
+{
+    const int dmax = (g.W - 1) / 2, q = lane & 3;
+    const float X0 = tx * kBwdTile - 0.5f, Y0 = ty * kBwdTile - 0.5f;
+    const float cx = (q == 1 || q == 2) ? X0 + kBwdTile : X0, cy = q >= 2 ? Y0 + kBwdTile : Y0;
+    const float oc = fmaf(cx, bv.cf, cy * bv.sf);
+    float tq = oc;
+    int bad = 0;
+    if (g.fan) {
+        const float qe = fmaf(cx, bv.sf, -cy * bv.cf) + g.dF;
+        bad = !(qe > 1e-3f * g.dF);
+        tq = g.dF * oc / qe;
+    }
+    float lo = tq, hi = tq;
+#pragma unroll
+    for (int o = 1; o <= 2; o <<= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    TileSpan sp;
+    const float inv = (float)(1.0 / g.dSize), lim = (float)dmax + 2.0f;
+    const int klo = max(__float2int_rd(fminf(fmaxf(lo * inv, -lim), lim)) - 1, -dmax);
+    const int khi = min(__float2int_ru(fminf(fmaxf(hi * inv, -lim), lim)) + 1, dmax);
+    sp.klo = klo;
+    sp.nseg = bad ? (1 << 20) : khi - klo + 1;
+    return sp;
+}
+
 __global__ void k_tile_span_max(const BwdParams p, int tiles, int *__restrict__ out)
 {
     int m = 0;
@@ -1157,9 +1189,11 @@ struct TiledSmem {
 };
 
 // Staging of one batch of VB base views for tile (tx, ty) (every thread of the
-// block takes part; ends with a block barrier): A, the tile's detector span
-// and centre per view; B1, the footprint coefficients of the staged
-// detectors; B2, their mirrored sinogram samples.
+// block takes part; ends with a block barrier), a warp per view: A, the
+// tile's detector span and centre in the view (every lane computes it, lane 0
+// keeps it for the pixels' pass); B1, the footprint coefficients of the staged
+// detectors; B2, their mirrored sinogram samples (a lane per detector: each
+// load instruction reads one sinogram row contiguously).
 template <bool FAN, int SEG, int VB>
 __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__restrict__ sino, int tx, int ty,
                                             double xc, double yc, int i0, int nb, TiledSmem<FAN, SEG, VB> &sm)
@@ -1170,15 +1204,12 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
     auto &rx = sm.rx;
     auto &seg = sm.seg;
     auto &seg2 = sm.seg2;
-    auto &tv = sm.tv;
-    auto &pfs = sm.pfs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, kWarps = blockDim.x >> 5;
     const int pC = g.pC;
-    // A: per view, the tile's detector span and centre
-    if (threadIdx.x < nb) {
-        const int iv = threadIdx.x;
+    for (int iv = warp; iv < nb; iv += kWarps) {
         const BwdView &bv = p.view[i0 + iv];
-        const TileSpan sp = tile_span(g, bv, tx, ty);
+        // A
+        const TileSpan sp = tile_span_lanes(g, bv, tx, ty, lane);
         TileView t;
         t.cT = bv.cf;
         t.sT = bv.sf;
@@ -1192,14 +1223,13 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
         t.AB = t.A * t.B;
         t.klo = sp.klo;
         t.nseg = min(sp.nseg, SEG);   // the plan chose SEG above every span
-        tv[iv] = t;
-        if (!FAN) pfs[iv] = make_footprint_v(bv.cf, bv.sf);
-    }
-    __syncthreads();
-    // B1: ray coefficients of the staged detectors, a warp per view
-    for (int iv = warp; iv < nb; iv += kWarps) {
-        const TileView &t = tv[iv];
+        const FootprintV pf = FAN ? FootprintV{} : make_footprint_v(bv.cf, bv.sf);
+        if (lane == 0) {
+            sm.tv[iv] = t;
+            if (!FAN) sm.pfs[iv] = pf;
+        }
         for (int kk = lane; kk < t.nseg; kk += 32) {
+            // B1
             const DetEntry &de = p.det[t.klo + kk + pC];
             if (FAN) {
                 const double D = fma(de.cB, t.uc - de.t, de.sB * t.vc);
@@ -1209,16 +1239,9 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
                 ra[FAN ? iv : 0][FAN ? kk : 0] = make_float4((float)D * f.iw, de.cBf * f.iw, de.sBf * f.iw, f.c1);
                 rb[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.hw, f.rho, 0.0f, 0.0f);
             } else {
-                rx[FAN ? 0 : iv][FAN ? 0 : kk] = (float)(t.uc - de.t) * pfs[iv].iw;
+                rx[FAN ? 0 : iv][FAN ? 0 : kk] = (float)(t.uc - de.t) * pf.iw;
             }
-        }
-    }
-    // B2: the mirrored sinogram samples, a warp per view, a lane per
-    // detector (each load instruction reads one sinogram row contiguously)
-    for (int iv = warp; iv < nb; iv += kWarps) {
-        const TileView &t = tv[iv];
-        const BwdView &bv = p.view[i0 + iv];
-        for (int kk = lane; kk < t.nseg; kk += 32) {
+            // B2
             const int dt = t.klo + kk;
             float v[8];
 #pragma unroll
@@ -1267,7 +1290,6 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     auto &seg2 = sm.seg2;
     auto &tv = sm.tv;
     auto &pfs = sm.pfs;
-    constexpr int kWarps = kBwdTile * kBwdTile / 32;
 
     if (p.zero_axes && tile == 0)
         for (int i = threadIdx.x; i < g.n; i += blockDim.x) {
@@ -1277,24 +1299,41 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     int tx, ty;
     decode_tile(tile, tx, ty);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // a warp takes an 8 x 4 block of the tile: compact blocks project onto
-    // fewer staged detectors than 16 x 2 rows, so each shared-memory read of
-    // a warp touches fewer distinct entries
+    // a warp takes an 8 x 4 block of the tile, each half-warp a 4 x 4 square.
+    // A 16-byte shared load costs a wavefront per 128 distinct bytes that a
+    // half-warp reads; the 16 pixels of a square project onto at most
+    // 3 sqrt(2) m + 1 consecutive staged detectors (m the magnification,
+    // below 1.3 here), so each such load of a half-warp reads at most eight
+    // 16-byte entries: one wavefront, against two for 8 x 2 rows
+#if CTPRJ_BWD_ROWS
     const int x = tx * kBwdTile + ((warp & 1) << 3) + (lane & 7);
     const int y = ty * kBwdTile + ((warp >> 1) << 2) + (lane >> 3);
+#else
+    const int x = tx * kBwdTile + ((warp & 1) << 3) + ((lane >> 4) << 2) + (lane & 3);
+    const int y = ty * kBwdTile + ((warp >> 1) << 2) + ((lane >> 2) & 3);
+#endif
     const bool valid = x <= g.half && y <= x;
     const int nimg = (y == 0 || y == x) ? 4 : 8;
     const double xc = tx * kBwdTile + 0.5 * (kBwdTile - 1), yc = ty * kBwdTile + 0.5 * (kBwdTile - 1);
     const float dx = (float)(x - xc), dy = (float)(y - yc);
-    const int dmax = (g.W - 1) / 2, pC = g.pC;
+    const int dmax = (g.W - 1) / 2;
     const float invdS = (float)(1.0 / g.dSize), dFs = (float)((double)g.dF / g.dSize);
     const float hbpar = 0.5f * g.beamWidthF;
     // fan beam: the half beam width at depth qe on ray B, over w, is
     // qe Kb (cos B / w) (prj/cpuPrj.c:254: bw = qe beamWidth cos B / d)
     const float Kb = FAN ? (float)(0.5 * g.beamWidth / g.d) : 0.0f;
-    float S[8];
+    // the eight sums, S[j] += w p[j], in pairs: one fma.rn.f32x2 for two
+    // sums (each rounded as one fmaf)
+    float2 S2[4];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) S[j] = 0.0f;
+    for (int j = 0; j < 4; ++j) S2[j] = make_float2(0.0f, 0.0f);
+    auto accumulate = [&](const float w, const float4 p0, const float4 p1) {
+        const float2 ww = make_float2(w, w);
+        S2[0] = __ffma2_rn(ww, make_float2(p0.x, p0.y), S2[0]);
+        S2[1] = __ffma2_rn(ww, make_float2(p0.z, p0.w), S2[1]);
+        S2[2] = __ffma2_rn(ww, make_float2(p1.x, p1.y), S2[2]);
+        S2[3] = __ffma2_rn(ww, make_float2(p1.z, p1.w), S2[3]);
+    };
 
     for (int i0 = 0; i0 < p.nv; i0 += VB) {
         const int nb = min(VB, p.nv - i0);
@@ -1335,27 +1374,10 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     }
 #pragma unroll
                     for (int q = 0; q < WIN; ++q) {
-                        const float4 p0 = seg[iv][0][k0 + q], p1 = seg[iv][1][k0 + q];
-                        S[0] = fmaf(w[q], p0.x, S[0]);
-                        S[1] = fmaf(w[q], p0.y, S[1]);
-                        S[2] = fmaf(w[q], p0.z, S[2]);
-                        S[3] = fmaf(w[q], p0.w, S[3]);
-                        S[4] = fmaf(w[q], p1.x, S[4]);
-                        S[5] = fmaf(w[q], p1.y, S[5]);
-                        S[6] = fmaf(w[q], p1.z, S[6]);
-                        S[7] = fmaf(w[q], p1.w, S[7]);
-                        if (!FAN) {
-                            const float4 r0 = seg2[FAN ? 0 : iv][0][FAN ? 0 : k0 + q];
-                            const float4 r1 = seg2[FAN ? 0 : iv][1][FAN ? 0 : k0 + q];
-                            S[0] = fmaf(w[q], r0.x, S[0]);
-                            S[1] = fmaf(w[q], r0.y, S[1]);
-                            S[2] = fmaf(w[q], r0.z, S[2]);
-                            S[3] = fmaf(w[q], r0.w, S[3]);
-                            S[4] = fmaf(w[q], r1.x, S[4]);
-                            S[5] = fmaf(w[q], r1.y, S[5]);
-                            S[6] = fmaf(w[q], r1.z, S[6]);
-                            S[7] = fmaf(w[q], r1.w, S[7]);
-                        }
+                        accumulate(w[q], seg[iv][0][k0 + q], seg[iv][1][k0 + q]);
+                        if (!FAN)
+                            accumulate(w[q], seg2[FAN ? 0 : iv][0][FAN ? 0 : k0 + q],
+                                       seg2[FAN ? 0 : iv][1][FAN ? 0 : k0 + q]);
                     }
                     continue;
                 }
@@ -1414,16 +1436,6 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     }
                     return w;
                 };
-                auto accumulate = [&](const float w, const float4 p0, const float4 p1) {
-                    S[0] = fmaf(w, p0.x, S[0]);
-                    S[1] = fmaf(w, p0.y, S[1]);
-                    S[2] = fmaf(w, p0.z, S[2]);
-                    S[3] = fmaf(w, p0.w, S[3]);
-                    S[4] = fmaf(w, p1.x, S[4]);
-                    S[5] = fmaf(w, p1.y, S[5]);
-                    S[6] = fmaf(w, p1.z, S[6]);
-                    S[7] = fmaf(w, p1.w, S[7]);
-                };
                 // two detectors per step, their shared-memory reads issued
                 // together (the second of an odd-length run re-reads dr and is
                 // skipped); per sum the order of the terms is unchanged
@@ -1444,6 +1456,12 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
             }
         }
         __syncthreads();
+    }
+    float S[8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        S[2 * j] = S2[j].x;
+        S[2 * j + 1] = S2[j].y;
     }
     if (valid) write_octant(p, img, x, y, nimg, S);
 }
