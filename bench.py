@@ -44,6 +44,16 @@ PARPRJ = dict(n=512, prjWidth=727, np=360)
 # the polychromatic model's own configuration: fan 1024^2, 720 views over
 # [0, 2 pi), 1024 detectors, source 2048 px from the isocentre
 BHC_WORKLOAD = dict(n=1024, prjWidth=1024, np=720, prjFull=720, dSize=1.0, effectiveRate=1.0, d=2048.0)
+# the projector alone on each configuration's geometry (--legs geometries):
+# (n, prjWidth, np, prjFull, dSize, effectiveRate, d)
+GEOMETRIES = {
+    "par256 (config 1)": (256, 363, 180, 360, 1.0, 1.0, 0.0),
+    "fan512 d=2048 (config 2)": (512, 1024, 360, 360, 1.0, 1.0, 2048.0),
+    "fan512 d=1024": (512, 512, 360, 360, 1.0, 1.0, 1024.0),
+    "fan1024 d=2048 (config 3)": (1024, 1024, 720, 720, 1.0, 1.0, 2048.0),
+    "par2048": (2048, 2048, 1440, 1440, 1.0, 1.0, 0.0),
+    "fan2048 d=8192 (config 5, headline)": (2048, 2048, 1440, 1440, 1.0, 1.0, 8192.0),
+}
 
 
 def geometry_tuple(w):
@@ -745,6 +755,46 @@ def issue_roof(prof, kname, kms, sm_mhz, updates):
             "source": "profiles/projector_counters.json (ncu smsp__inst_executed.sum)"}
 
 
+def geometries_arm(args):
+    """Forward and backprojection times per geometry (CUDA events around each
+    launch on the launching stream, the 512 MiB L2 flush before each; median
+    of --steps launches after --warmup), one GPU."""
+    import torch
+    import imgrecsrc_b200 as ct
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    out = {}
+    for name, t in GEOMETRIES.items():
+        g = ct.Geometry(*t)
+        pr = ct.Projector(g)
+        x = torch.rand(g.n, g.n, device="cuda", generator=gen)
+        y = torch.rand(g.np, g.prjWidth, device="cuda", generator=gen)
+        s = torch.empty(g.np, g.prjWidth, device="cuda")
+        b = torch.empty(g.n, g.n, device="cuda")
+        res = {}
+        for kind in ("fwd_ms", "bwd_ms"):
+            ts = []
+            for it in range(max(3, args.warmup) + args.steps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                if kind == "fwd_ms":
+                    pr.forward(x, out=s)
+                else:
+                    pr.backward(y, out=b)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if it >= max(3, args.warmup):
+                    ts.append(e0.elapsed_time(e1))
+            res[kind] = round(statistics.median(ts), 4)
+        out[name] = res
+        pr.close()
+    print(json.dumps({"geometries": out, "steps": args.steps, "warmup": max(3, args.warmup),
+                      "timing": "CUDA events per launch, L2 flushed before each, median"}), flush=True)
+
+
 def shared_roof(prof, kname, kms, sm_mhz):
     """The shared-memory roof of the staged backprojection: its shared-memory
     wavefronts per launch (ncu l1tex__data_pipe_lsu_wavefronts_mem_shared.sum)
@@ -824,8 +874,9 @@ def main():
     ap.add_argument("--loop-geometry", default="2048", choices=["2048", "1024"],
                     help="reconstruction leg on the 2048^2 workload (config 5) or on the "
                          "1024^2 configuration of the polychromatic model (smaller, for profiling)")
-    ap.add_argument("--legs", default="all", choices=["all", "projector"],
-                    help="projector: the headline step and its end-to-end run only (for profiling)")
+    ap.add_argument("--legs", default="all", choices=["all", "projector", "geometries"],
+                    help="projector: the headline step and its end-to-end run only (for profiling); "
+                         "geometries: forward and backprojection times on each configuration's geometry")
     ap.add_argument("--selftest", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.gpus < 1:
@@ -834,6 +885,8 @@ def main():
         sys.exit(relaunch(args, sys.argv[1:]))
     if args.selftest:
         selftest_arm(args)
+    elif args.legs == "geometries":
+        geometries_arm(args)
     elif args.impl == "reference":
         reference_arm(args)
     else:
