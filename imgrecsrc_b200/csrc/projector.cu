@@ -208,6 +208,12 @@ __device__ __forceinline__ FwdRay fwd_ray(const FwdParams &p, int b, int k)
 // The rays of one forward block: V adjacent base views (one per warp) x 32
 // adjacent detectors; block (bx, by) of the per-plan grid.  Returns this
 // thread's Poisson terms in polychromatic mode.
+// Build-time variant CTPRJ_FWD_WARP_VIEWS = G > 1: a warp takes G adjacent
+// views x 32 / G detectors instead (measured slower: G unaligned pixel runs per
+// gather touch more 128-byte lines than one contiguous run of 32 rays).
+#ifndef CTPRJ_FWD_WARP_VIEWS
+#define CTPRJ_FWD_WARP_VIEWS 1
+#endif
 template <bool FAN, int MODE, int V>
 __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int by,
                                                const float4 *__restrict__ quad,
@@ -216,8 +222,10 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
                                                const double *tab, const double *Ie)
 {
     const Geo &g = p.g;
-    const int b = bx * V + (int)(threadIdx.x >> 5);
-    const int r = by * 32 + (int)(threadIdx.x & 31);
+    constexpr int G = V < CTPRJ_FWD_WARP_VIEWS ? V : CTPRJ_FWD_WARP_VIEWS, D = 32 / G;
+    const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31);
+    const int b = bx * V + (warp / G) * G + lane / D;
+    const int r = by * 32 + (warp % G) * D + lane % D;
     double fsum = 0.0;            // polychromatic mode: this thread's Poisson terms
     // detector 0 of an even-width sinogram: no ray, zero projection
     if (MODE != kModeCount && p.zero_col0 && bx == 0 && by == 0)
@@ -234,7 +242,8 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
     // needs: xr - xl is affine in y, so a ray's widest run is at the first or
     // the last row.  Every lane of the (full) warp takes part in the maximum,
     // lanes without a ray with 0, so the choice depends on the warp's rays
-    // alone and a batched launch makes the same one.
+    // alone and a batched launch makes the same one (the variant with G views
+    // per warp takes it per view, over that view's lanes).
     const bool live = b < p.nb && r < p.nk;
     const int k = p.k0 + r;
     FwdRay ray = {};
@@ -248,7 +257,12 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
             wcode = wmax < 1.95f ? 3 : (wmax < 2.95f ? 4 : 5);
         }
     }
-    wcode = __reduce_max_sync(0xffffffffu, wcode);
+    if (G == 1) {
+        wcode = __reduce_max_sync(0xffffffffu, wcode);
+    } else {
+#pragma unroll
+        for (int o = 1; o < D; o <<= 1) wcode = max(wcode, __shfl_xor_sync(0xffffffffu, wcode, o));
+    }
     if (live) {
         const double cR = ray.cR, sR = ray.sR, off = ray.off;
         const float Alf = ray.Al, Slf = ray.Sl, Arf = ray.Ar, Srf = ray.Sr;
