@@ -385,6 +385,19 @@ __device__ __forceinline__ double forward_rays(const FwdParams &p, int bx, int b
             if (xc < -(float)half - 2.0f || xc > (float)half + 2.0f) return;
             int xs = (WN == 3 ? __float2int_rn(xc) : __float2int_rd(xc)) - 1;
             xs = min(max(xs, -half), half - (WN - 1));
+#if CTPRJ_FWD_PREFETCH
+            // Build-time variant: ask L1 for the quad lines this ray will read
+            // CTPRJ_FWD_PREFETCH rows further on (at this row's x: the run
+            // moves less than a pixel per row), where that row is in the image
+            {
+                constexpr int PD = CTPRJ_FWD_PREFETCH;
+                if (NEG ? PD - y <= half : y - PD >= 0) {
+                    const float4 *qa = NEG ? q + PD * QW : q - PD * QW;
+                    asm volatile("prefetch.L1 [%0];" ::"l"(qa + xs));
+                    asm volatile("prefetch.L1 [%0];" ::"l"(qa - xs));
+                }
+            }
+#endif
             const float r0 = (float)fma((double)xs, cR, fma((double)y, sR, -off)) * fp.iw;
             const float hb0 = (FAN ? 0.5f * fmaf(fmaf((float)xs, sTf, -yf * cTf), kbw, bwc)
                                    : 0.5f * g.beamWidthF) * fp.iw;
