@@ -352,6 +352,21 @@ def our_arm(args):
     e2e_t = max_over_ranks(statistics.mean(e2e_times), pg, "cuda")
     e2e_val = replica_value(world, nnz_f + nnz_b, e2e_t * 1e3)
     img_b, sino_b = 4 * g.n * g.n, 4 * g.np * g.prjWidth
+    # the same calls on pageable host buffers (the reference gateway's malloc'd
+    # arrays, prj/mPrj.c:70-73), for the record
+    p_img = np.ascontiguousarray(h_img.numpy().copy())
+    p_sino = np.empty((g.np, g.prjWidth), np.float32)
+    p_back = np.empty((g.n, g.n), np.float32)
+    pageable_times = []
+    for it in range(2 + min(args.steps, 5)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ct.check(L.gpuPrj(ctypes.c_void_p(p_img.ctypes.data), ctypes.c_void_p(p_sino.ctypes.data), bytes([ct.FWD_BIT])))
+        ct.check(L.gpuPrj(ctypes.c_void_p(p_back.ctypes.data), ctypes.c_void_p(p_sino.ctypes.data), bytes([ct.BWD_BIT])))
+        if it >= 2:
+            pageable_times.append(time.perf_counter() - t0)
+    pageable_t = max_over_ranks(statistics.mean(pageable_times), pg, "cuda")
 
     line = {
         "metric": METRIC, "value": value, "unit": "Gray-px/s", "n_gpus": world,
@@ -368,7 +383,7 @@ def our_arm(args):
                      "bytes_per_launch": kbytes, "bytes_rule": "4 B per nonzero update + image + sinogram"},
         "e2e": {"value": e2e_val, "unit": "Gray-px/s", "h2d_bytes_per_step": img_b + sino_b,
                 "d2h_bytes_per_step": sino_b + img_b, "api": "setup()/gpuPrj() C ABI, pinned host buffers",
-                "ms_per_step": e2e_t * 1e3},
+                "ms_per_step": e2e_t * 1e3, "pageable_ms_per_step": pageable_t * 1e3},
         "gpu_launches": 3 * args.steps,
         "clocks": clk,
     }
