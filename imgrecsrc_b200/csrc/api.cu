@@ -5,8 +5,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
+#include <condition_variable>
 #include <mutex>
+#include <thread>
 #include <vector>
+
+#include <unistd.h>
 
 #include "ctprj_internal.h"
 #include "footprint.cuh"
@@ -345,6 +350,10 @@ struct prjConf *pConf = &g_conf;
 }
 static ctprj_plan *g_plan = nullptr;
 static float *g_dimg = nullptr, *g_dsino = nullptr;
+// page-locked, mapped staging for pageable caller buffers (allocated on first
+// use, as large as the larger of the image and the sinogram)
+static float *g_stage = nullptr;
+static size_t g_stage_bytes = 0;
 static int g_status = CTPRJ_ENOTSETUP;
 static char g_msg[512] = "setup() has not been called";
 
@@ -377,11 +386,123 @@ static void release_global()
         DeviceGuard dg(g_plan->device);
         cudaFree(g_dimg);
         cudaFree(g_dsino);
+        if (g_stage) cudaFreeHost(g_stage);
         free_plan(g_plan);
     }
     g_plan = nullptr;
     g_dimg = g_dsino = nullptr;
+    g_stage = nullptr;
+    g_stage_bytes = 0;
 }
+
+// Host copies of pageable caller buffers to and from the staging buffer, split
+// over a few threads: one thread copies at about a quarter of what four reach
+// (a driver-staged copy of pageable memory runs at about 20 GB/s, four host
+// threads into page-locked memory at about 60).  The workers are started on
+// first use and parked between copies; the calling thread takes a share.
+class HostCopier {
+public:
+    static HostCopier &get()
+    {
+        static HostCopier c;
+        return c;
+    }
+    // Copies `bytes` from src to dst, each thread (the workers and the caller)
+    // its own contiguous share in pieces of at most `piece` bytes; after each
+    // piece, sent(offset, length) when given (called from that thread; its
+    // nonzero return is kept and returned).  The next job starts only when
+    // each worker has reported this one.
+    using Sent = int (*)(void *ctx, size_t offset, size_t length);
+    int copy(void *dst, const void *src, size_t bytes, size_t piece = 0, Sent sent = nullptr,
+             void *ctx = nullptr)
+    {
+        Job j = {(char *)dst, (const char *)src, bytes, workers_.size() + 1, piece ? piece : bytes, sent, ctx};
+        // small copies, and a forked child (which has none of the parent's
+        // workers), stay on the calling thread
+        if (j.parts == 1 || bytes < (2u << 20) || getpid() != pid_) {
+            j.parts = 1;
+            return part(j, 0);
+        }
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            job_ = j;
+            done_ = 0;
+            status_ = 0;
+            ++gen_;
+        }
+        cv_.notify_all();
+        const int mine = part(j, 0);
+        std::unique_lock<std::mutex> lk(m_);
+        done_cv_.wait(lk, [&] { return done_ == workers_.size(); });
+        return mine ? mine : status_;
+    }
+    ~HostCopier()
+    {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : workers_) t.join();
+    }
+
+private:
+    struct Job {
+        char *dst;
+        const char *src;
+        size_t bytes, parts, piece;
+        Sent sent;
+        void *ctx;
+    };
+    HostCopier()
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const unsigned n = hw >= 8 ? 3 : (hw >= 4 ? 1 : 0);   // plus the caller
+        for (unsigned i = 0; i < n; ++i) workers_.emplace_back([this, i] { loop(i + 1); });
+        pid_ = getpid();
+    }
+    static int part(const Job &j, size_t i)
+    {
+        const size_t a = j.bytes * i / j.parts, b = j.bytes * (i + 1) / j.parts;
+        int st = 0;
+        for (size_t o = a; o < b && !st; o += j.piece) {
+            const size_t len = std::min(j.piece, b - o);
+            memcpy(j.dst + o, j.src + o, len);
+            if (j.sent) st = j.sent(j.ctx, o, len);
+        }
+        return st;
+    }
+    void loop(size_t idx)
+    {
+        unsigned seen = 0;
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                j = job_;
+            }
+            const int st = part(j, idx);
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                if (st && !status_) status_ = st;
+                ++done_;
+            }
+            done_cv_.notify_one();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex m_;
+    std::condition_variable cv_, done_cv_;
+    Job job_ = {nullptr, nullptr, 0, 1, 1, nullptr, nullptr};
+    size_t done_ = 0;
+    int status_ = 0;
+    unsigned gen_ = 0;
+    bool stop_ = false;
+    pid_t pid_ = 0;
+};
 
 extern "C" void setup(int n, int prjWidth, int np, int prjFull, float dSize, float effectiveRate,
                       float d)
@@ -444,10 +565,52 @@ static float *mapped_alias(void *host)
     return a.type == cudaMemoryTypeHost ? (float *)a.devicePointer : nullptr;
 }
 
+// The staging buffer, grown to at least `bytes` (g_mu held)
+static int stage(size_t bytes)
+{
+    if (g_stage_bytes >= bytes) return CTPRJ_OK;
+    if (g_stage) cudaFreeHost(g_stage);
+    g_stage = nullptr;
+    g_stage_bytes = 0;
+    int st = cuda_error(cudaHostAlloc((void **)&g_stage, bytes, cudaHostAllocMapped), "staging buffer");
+    if (!st) g_stage_bytes = bytes;
+    return st;
+}
+
+// Upload of a caller buffer: straight from page-locked memory, or through the
+// staging buffer, each 1 MiB piece sent as soon as it has been copied in (the
+// host threads copy while the copy engine sends).  The device and stream of a
+// piece's transfer are the calling thread's: every thread sets the device.
+struct UploadCtx {
+    char *dev;
+    const char *stage;
+    cudaStream_t s;
+    int device;
+};
+
+static int send_piece(void *p, size_t off, size_t len)
+{
+    const UploadCtx &u = *(const UploadCtx *)p;
+    if (cudaSetDevice(u.device) != cudaSuccess) return cuda_error(cudaGetLastError(), "upload device");
+    return cuda_error(cudaMemcpyAsync(u.dev + off, u.stage + off, len, cudaMemcpyHostToDevice, u.s), "upload");
+}
+
+static int upload(float *dev, const float *host, size_t bytes, cudaStream_t s, const char *what)
+{
+    if (mapped_alias((void *)host)) return cuda_error(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s), what);
+    int st = stage(std::max(sizeof(float) * g_conf.imgSize, sizeof(float) * g_conf.sinoSize));
+    if (st) return st;
+    UploadCtx u = {(char *)dev, (const char *)g_stage, s, g_plan->device};
+    st = HostCopier::get().copy(g_stage, host, bytes, 1u << 20, send_piece, &u);
+    // the failing piece's message is on the thread that sent it
+    return st ? set_error(st, "%s: a host-to-device copy failed", what) : CTPRJ_OK;
+}
+
 // prj/gpuPrj.cu:899-958: upload the input, run the pass, download the result,
-// return when the result is in the caller's buffer.  When the result buffer is
-// page-locked the kernel writes it directly over the bus as it produces it, so
-// the download overlaps the pass instead of following it.
+// return when the result is in the caller's buffer.  The result goes straight
+// over the bus into page-locked memory as the kernel produces it: the caller's
+// buffer when it is page-locked, else the staging buffer (after the input has
+// left it), copied out by the host threads when the pass is done.
 extern "C" int gpuPrj(float *img, float *sino, char cmd)
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -458,25 +621,34 @@ extern "C" int gpuPrj(float *img, float *sino, char cmd)
     const size_t ib = sizeof(float) * g_conf.imgSize, sb = sizeof(float) * g_conf.sinoSize;
     cudaStream_t s = 0;
     int st;
+    float *result = nullptr;   // the caller's pageable result buffer
+    size_t rb = 0;
     if (cmd & FWD_BIT) {
         float *out = mapped_alias(sino);
-        if ((st = cuda_error(cudaMemcpyAsync(g_dimg, img, ib, cudaMemcpyHostToDevice, s), "image upload")) ||
-            (st = ctprj_forward(g_plan, g_dimg, out ? out : g_dsino, s)))
-            return st;
-        if (!out && (st = cuda_error(cudaMemcpyAsync(sino, g_dsino, sb, cudaMemcpyDeviceToHost, s),
-                                     "sinogram download")))
-            return st;
+        if ((st = upload(g_dimg, img, ib, s, "image upload"))) return st;
+        if (!out) {
+            if ((st = stage(std::max(ib, sb)))) return st;
+            out = mapped_alias(g_stage);
+            result = sino;
+            rb = sb;
+        }
+        if ((st = ctprj_forward(g_plan, g_dimg, out, s))) return st;
     } else if (cmd & (BWD_BIT | FBP_BIT)) {
         float *out = mapped_alias(img);
-        if ((st = cuda_error(cudaMemcpyAsync(g_dsino, sino, sb, cudaMemcpyHostToDevice, s), "sinogram upload")) ||
-            (st = (cmd & BWD_BIT) ? ctprj_backward(g_plan, g_dsino, out ? out : g_dimg, s)
-                                  : ctprj_fbp_device(g_plan, g_dsino, out ? out : g_dimg, s)))
-            return st;
-        if (!out && (st = cuda_error(cudaMemcpyAsync(img, g_dimg, ib, cudaMemcpyDeviceToHost, s),
-                                     "image download")))
+        if ((st = upload(g_dsino, sino, sb, s, "sinogram upload"))) return st;
+        if (!out) {
+            if ((st = stage(std::max(ib, sb)))) return st;
+            out = mapped_alias(g_stage);
+            result = img;
+            rb = ib;
+        }
+        if ((st = (cmd & BWD_BIT) ? ctprj_backward(g_plan, g_dsino, out, s)
+                                  : ctprj_fbp_device(g_plan, g_dsino, out, s)))
             return st;
     } else {
         return CTPRJ_OK;   // the reference does nothing for other commands
     }
-    return cuda_error(cudaStreamSynchronize(s), "gpuPrj synchronize");
+    if ((st = cuda_error(cudaStreamSynchronize(s), "gpuPrj synchronize"))) return st;
+    if (result) HostCopier::get().copy(result, g_stage, rb);
+    return CTPRJ_OK;
 }

@@ -43,3 +43,36 @@ def test_pageable_equals_pinned():
     # and the device path agrees
     pr = ct.Projector(ct.Geometry(n, W, npv, npv, 1.0, 1.0, 7000.0))
     assert np.array_equal(pr.forward(torch.from_numpy(img_u).cuda()).cpu().numpy(), sino_u)
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data if isinstance(a, np.ndarray) else a.data_ptr())
+
+
+def test_mixed_buffers_fbp_and_a_new_setup():
+    """Pageable input with a pinned result and the other way round, FBP, and
+    a second setup() with larger buffers (the staging buffer of pageable calls
+    grows with it): every combination gives the pinned path's bits."""
+    L = ct.lib()
+    rng = np.random.default_rng(9)
+    for n, W, npv, d in ((300, 431, 240, 900.0), (1100, 1500, 720, 4000.0)):
+        L.setup(n, W, npv, npv, 1.0, 1.0, d)
+        img_u = phantom.ellipse_phantom(n, seed=n)
+        y_u = rng.standard_normal((npv, W)).astype(np.float32)
+        img_p, y_p = torch.from_numpy(img_u).pin_memory(), torch.from_numpy(y_u).pin_memory()
+        ref_s, ref_b, ref_f = torch.empty(npv, W).pin_memory(), torch.empty(n, n).pin_memory(), torch.empty(n, n).pin_memory()
+        ct.check(L.gpuPrj(_ptr(img_p), _ptr(ref_s), bytes([ct.FWD_BIT])))
+        ct.check(L.gpuPrj(_ptr(ref_b), _ptr(y_p), bytes([ct.BWD_BIT])))
+        ct.check(L.gpuPrj(_ptr(ref_f), _ptr(y_p), bytes([ct.FBP_BIT])))
+        for src_img, src_y in ((img_u, y_p), (img_p, y_u), (img_u, y_u)):
+            for pinned_out in (False, True):
+                s_out = torch.empty(npv, W).pin_memory() if pinned_out else np.full((npv, W), np.nan, np.float32)
+                b_out = torch.empty(n, n).pin_memory() if pinned_out else np.full((n, n), np.nan, np.float32)
+                f_out = torch.empty(n, n).pin_memory() if pinned_out else np.full((n, n), np.nan, np.float32)
+                ct.check(L.gpuPrj(_ptr(src_img), _ptr(s_out), bytes([ct.FWD_BIT])))
+                ct.check(L.gpuPrj(_ptr(b_out), _ptr(src_y), bytes([ct.BWD_BIT])))
+                ct.check(L.gpuPrj(_ptr(f_out), _ptr(src_y), bytes([ct.FBP_BIT])))
+                as_np = lambda a: a.numpy() if isinstance(a, torch.Tensor) else a
+                assert np.array_equal(as_np(s_out), ref_s.numpy()), (n, pinned_out)
+                assert np.array_equal(as_np(b_out), ref_b.numpy()), (n, pinned_out)
+                assert np.array_equal(as_np(f_out), ref_f.numpy()), (n, pinned_out)
