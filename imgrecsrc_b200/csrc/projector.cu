@@ -1326,12 +1326,11 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
     int tx, ty;
     decode_tile(tile, tx, ty);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // a warp takes an 8 x 4 block of the tile, each half-warp a 4 x 4 square.
-    // A 16-byte shared load costs a wavefront per 128 distinct bytes that a
-    // half-warp reads; the 16 pixels of a square project onto at most
-    // 3 sqrt(2) m + 1 consecutive staged detectors (m the magnification,
-    // below 1.3 here), so each such load of a half-warp reads at most eight
-    // 16-byte entries: one wavefront, against two for 8 x 2 rows
+    // a warp takes an 8 x 4 block of the tile, each half-warp a 4 x 4 square:
+    // the 16 pixels of a square project onto at most 3 sqrt(2) m + 1
+    // consecutive staged detectors (m the magnification), fewer than the
+    // eight 16-byte entries that share no bank, so a half-warp's window loads
+    // never conflict (8 x 2 rows do)
 #if CTPRJ_BWD_ROWS
     const int x = tx * kBwdTile + ((warp & 1) << 3) + (lane & 7);
     const int y = ty * kBwdTile + ((warp >> 1) << 2) + (lane >> 3);
