@@ -48,6 +48,13 @@ namespace ctprj {
 #ifndef CTPRJ_BWD_MINBLOCKS
 #define CTPRJ_BWD_MINBLOCKS 4
 #endif
+// CTPRJ_BWD_DERIVE = 1: the staged fan backprojection keeps one coefficient
+// plane per detector and derives the footprint's hw and w / (2 b1) from its
+// b2 / w (two reciprocals) instead of reading them from a second plane
+#ifndef CTPRJ_BWD_DERIVE
+#define CTPRJ_BWD_DERIVE 0
+#endif
+constexpr bool kBwdDerive = CTPRJ_BWD_DERIVE != 0;
 constexpr int kFwdViews = CTPRJ_FWD_VIEWS;
 constexpr int kFwdThreads = 32 * kFwdViews;
 constexpr int kBwdTile = 16;   // 16 x 16 octant pixels per block
@@ -1204,7 +1211,7 @@ struct TiledSmem {
     // (measured faster than a packed 8-byte plane: 4.70 against 4.75 ms at the
     // 2048^2 fan workload, 0.90 against 1.00 ms at 1024^2 with d = 2048)
     float4 ra[FAN ? VB : 1][FAN ? SEG : 1];
-    float4 rb[FAN ? VB : 1][FAN ? SEG : 1];
+    float4 rb[FAN && !kBwdDerive ? VB : 1][FAN && !kBwdDerive ? SEG : 1];
     float rx[FAN ? 1 : VB][FAN ? 1 : SEG];
     // the eight (sixteen) mirrored samples of a staged ray as two (four)
     // float4 planes: two (four) 16-byte reads per detector and pixel, and
@@ -1214,6 +1221,27 @@ struct TiledSmem {
     TileView tv[VB];
     FootprintV pfs[VB];
 };
+
+// The footprint numbers of a staged fan detector.  All three follow from
+// t = lo / hi of the ray's direction: b2 / w = (1 + t) / (2 t), hw = t / 2 =
+// 1 / (4 b2/w - 2) and w / (2 b1) = t / (1 - t) = 1 / (2 b2/w - 2).  The
+// derived pair also holds where make_footprint_v floors a zero width: for
+// w = 0, hw comes out ~1e-31 (it multiplies a bounded term) and w / (2 b1)
+// matches the floored ratio; for b1 = 0 the floor below keeps the ratio
+// finite.  Each is within ~1e-7 of the stored value's effect on a weight.
+__device__ __forceinline__ FootprintV staged_footprint(const float4 a, const float4 &b)
+{
+    FootprintV f;
+    f.c1 = a.w;
+    if (kBwdDerive) {
+        f.hw = __fdividef(1.0f, fmaf(4.0f, a.w, -2.0f));
+        f.rho = __fdividef(1.0f, fmaxf(fmaf(2.0f, a.w, -2.0f), 1e-30f));
+    } else {
+        f.hw = b.x;
+        f.rho = b.y;
+    }
+    return f;
+}
 
 // Staging of one batch of VB base views for tile (tx, ty) (every thread of the
 // block takes part; ends with a block barrier), a warp per view: A, the
@@ -1264,7 +1292,8 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
                 const float sR = fmaf(de.sBf, t.cT, de.cBf * t.sT);
                 const FootprintV f = make_footprint_v(cR, sR);
                 ra[FAN ? iv : 0][FAN ? kk : 0] = make_float4((float)D * f.iw, de.cBf * f.iw, de.sBf * f.iw, f.c1);
-                rb[FAN ? iv : 0][FAN ? kk : 0] = make_float4(f.hw, f.rho, 0.0f, 0.0f);
+                if (!kBwdDerive)
+                    rb[FAN && !kBwdDerive ? iv : 0][FAN && !kBwdDerive ? kk : 0] = make_float4(f.hw, f.rho, 0.0f, 0.0f);
             } else {
                 rx[FAN ? 0 : iv][FAN ? 0 : kk] = (float)(t.uc - de.t) * pf.iw;
             }
@@ -1386,12 +1415,9 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     for (int q = 0; q < WIN; ++q) {
                         if (FAN) {
                             const float4 a = ra[FAN ? iv : 0][FAN ? k0 + q : 0];
-                            const float4 b = rb[FAN ? iv : 0][FAN ? k0 + q : 0];
                             const float D = fmaf(a.y, du, fmaf(a.z, dv, a.x));
-                            FootprintV f;
-                            f.hw = b.x;
-                            f.c1 = a.w;
-                            f.rho = b.y;
+                            const FootprintV f = staged_footprint(a, rb[FAN && !kBwdDerive ? iv : 0]
+                                                                        [FAN && !kBwdDerive ? k0 + q : 0]);
                             w[q] = footprint_weight_v(D, qeK * a.y, f);
                             if (FBP) w[q] *= fbpw;
                         } else {
@@ -1449,12 +1475,9 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     float w;
                     if (FAN) {
                         const float4 a = ra[FAN ? iv : 0][FAN ? kk : 0];
-                        const float4 b = rb[FAN ? iv : 0][FAN ? kk : 0];
                         const float D = fmaf(a.y, du, fmaf(a.z, dv, a.x));
-                        FootprintV f;
-                        f.hw = b.x;
-                        f.c1 = a.w;
-                        f.rho = b.y;
+                        const FootprintV f = staged_footprint(a, rb[FAN && !kBwdDerive ? iv : 0]
+                                                                    [FAN && !kBwdDerive ? kk : 0]);
                         w = footprint_weight_v(D, qeK * a.y, f);
                         if (FBP) w *= fbpw;
                     } else {
@@ -1557,11 +1580,7 @@ k_backward_pair(const BwdParams p, const float *__restrict__ sino, float *__rest
             auto slot = [&](const int kk) {
                 if ((unsigned)kk >= (unsigned)t.nseg) return;
                 const float4 a = sm.ra[iv][kk];
-                const float4 b = sm.rb[iv][kk];
-                FootprintV f;
-                f.hw = b.x;
-                f.c1 = a.w;
-                f.rho = b.y;
+                const FootprintV f = staged_footprint(a, sm.rb[kBwdDerive ? 0 : iv][kBwdDerive ? 0 : kk]);
                 float w1 = footprint_weight_v(fmaf(a.y, du1, fmaf(a.z, dv1, a.x)), (qe1 * Kb) * a.y, f);
                 float w2 = footprint_weight_v(fmaf(a.y, du2, fmaf(a.z, dv2, a.x)), (qe2 * Kb) * a.y, f);
                 if (FBP) {
