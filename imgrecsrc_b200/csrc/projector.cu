@@ -55,6 +55,12 @@ namespace ctprj {
 #define CTPRJ_BWD_DERIVE 0
 #endif
 constexpr bool kBwdDerive = CTPRJ_BWD_DERIVE != 0;
+// CTPRJ_BWD_ASYNC = 1: the staged backprojection copies its mirrored sinogram
+// samples into shared memory by 4-byte cp.async (no register round trip; the
+// lane computes the ray coefficients while they are in flight)
+#ifndef CTPRJ_BWD_ASYNC
+#define CTPRJ_BWD_ASYNC 0
+#endif
 constexpr int kFwdViews = CTPRJ_FWD_VIEWS;
 constexpr int kFwdThreads = 32 * kFwdViews;
 constexpr int kBwdTile = 16;   // 16 x 16 octant pixels per block
@@ -1222,6 +1228,15 @@ struct TiledSmem {
     FootprintV pfs[VB];
 };
 
+// one float from global into shared memory without a register round trip;
+// an invalid source reads nothing and writes zero
+__device__ __forceinline__ void stage_async4(float *smem, const float *gmem, bool valid)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+
 // The footprint numbers of a staged fan detector.  All three follow from
 // t = lo / hi of the ray's direction: b2 / w = (1 + t) / (2 t), hw = t / 2 =
 // 1 / (4 b2/w - 2) and w / (2 b1) = t / (1 - t) = 1 / (2 b2/w - 2).  The
@@ -1283,6 +1298,27 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
             sm.tv[iv] = t;
             if (!FAN) sm.pfs[iv] = pf;
         }
+#if CTPRJ_BWD_ASYNC
+        // B2 first, asynchronously: the same samples as below, in flight while
+        // B1 runs; the block barrier at the end follows a wait for them
+        for (int kk = lane; kk < t.nseg; kk += 32) {
+            const int dt = t.klo + kk;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const int row = bv.row[j];
+                stage_async4(&seg[iv][j >> 2][kk].x + (j & 3),
+                             sino + (row >= 0 ? row + pC + (j < 4 ? dt : -dt) : 0), row >= 0);
+            }
+            if (!FAN) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int row2 = bv.row2[j];
+                    stage_async4(&seg2[FAN ? 0 : iv][j >> 2][FAN ? 0 : kk].x + (j & 3),
+                                 sino + (row2 >= 0 ? row2 + pC - (j < 4 ? dt : -dt) : 0), row2 >= 0);
+                }
+            }
+        }
+#endif
         for (int kk = lane; kk < t.nseg; kk += 32) {
             // B1
             const DetEntry &de = p.det[t.klo + kk + pC];
@@ -1297,6 +1333,7 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
             } else {
                 rx[FAN ? 0 : iv][FAN ? 0 : kk] = (float)(t.uc - de.t) * pf.iw;
             }
+#if !CTPRJ_BWD_ASYNC
             // B2
             const int dt = t.klo + kk;
             float v[8];
@@ -1316,8 +1353,12 @@ __device__ __forceinline__ void stage_batch(const BwdParams &p, const float *__r
                 seg2[FAN ? 0 : iv][0][FAN ? 0 : kk] = make_float4(v[0], v[1], v[2], v[3]);
                 seg2[FAN ? 0 : iv][1][FAN ? 0 : kk] = make_float4(v[4], v[5], v[6], v[7]);
             }
+#endif
         }
     }
+#if CTPRJ_BWD_ASYNC
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+#endif
     __syncthreads();
 }
 
