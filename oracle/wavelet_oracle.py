@@ -202,6 +202,14 @@ def l1_penalty(x, h, L, maskk=None):
     return float(y.sum())
 
 
+def circular_mask(n, m=None):
+    """Utils.getCircularMask(n, m) (utils/Utils.m:438-444): the pixels whose
+    0-based coordinates lie closer than m/2 - 1 to (n/2, n/2)."""
+    m = n if m is None else m
+    x, y = np.meshgrid(np.arange(n), np.arange(n))
+    return np.sqrt((x - n / 2) ** 2 + (y - n / 2) ** 2) < (m / 2 - 1)
+
+
 def wvlt_mask(mask, h, L):
     """maskk = wvltMask(Mask, dwt_L, daub) (utils/wvltMask.m), as there: the
     union over the mask's pixels e_i of Wt(e_i) != 0."""

@@ -17,6 +17,7 @@ from imgrecsrc_b200 import wavelet  # noqa: E402
 from imgrecsrc_b200._lib import CtprjError  # noqa: E402
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rwt_golden.npz")
+MASKS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "wvltmask_golden.npz")
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -246,6 +247,23 @@ def test_wvlt_mask_matches_utils_wvltmask(daub, L):
     h = W.daubcqf(daub)
     g = wavelet.wvlt_mask(torch.from_numpy(m).cuda(), h, L).cpu().numpy().astype(bool)
     assert np.array_equal(g, W.wvlt_mask(m, h, L))
+
+
+def test_wvlt_mask_matches_every_reference_mask():
+    """ctprj_wvlt_mask on Utils.getCircularMask(n) against all 19 coefficient
+    masks the reference ships (utils/MaskWvlt<n>CircleL<L>D<D>.mat, outputs of
+    its utils/wvltMask.m; n = 64 ... 1024, 1 to 9 levels, Haar and the 6-tap
+    filter), bit for bit."""
+    z = np.load(MASKS)
+    keys = sorted(k for k in z.files if not k.endswith("_count"))
+    assert len(keys) == 19
+    for key in keys:
+        n, L, D = (int(p[1:]) for p in key.split("_"))
+        ref = np.unpackbits(z[key], count=n * n).reshape((n, n), order="F").astype(bool)
+        assert ref.sum() == int(z[key + "_count"])
+        m = torch.from_numpy(W.circular_mask(n).astype(np.uint8)).cuda()
+        got = wavelet.wvlt_mask(m, W.daubcqf(D), L).cpu().numpy().astype(bool)
+        assert np.array_equal(got, ref), (key, int((got != ref).sum()))
 
 
 @pytest.mark.parametrize("method,proximal,daub", [("npg", "wvltADMM", 2), ("pg", "wvltADMM", 4),

@@ -13,6 +13,15 @@ import pytest
 from oracle import wavelet_oracle as W
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rwt_golden.npz")
+MASKS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "wvltmask_golden.npz")
+
+
+def reference_mask(z, key):
+    """(n, L, daub) and the mask of golden entry `key` (MATLAB's element order)."""
+    n, L, D = (int(p[1:]) for p in key.split("_"))
+    m = np.unpackbits(z[key], count=n * n).reshape((n, n), order="F").astype(bool)
+    assert m.sum() == int(z[key + "_count"])
+    return n, L, D, m
 
 
 def test_daubechies_filters():
@@ -153,3 +162,15 @@ def test_masked_admm_keeps_the_masks():
         xb = 2 * xn - x
         x = xn
     assert np.linalg.norm(al - x) / np.linalg.norm(x) < 1e-3
+
+
+@pytest.mark.parametrize("key", ["n64_L3_D2", "n128_L2_D2", "n128_L6_D6"])
+def test_wavelet_mask_matches_the_reference_masks(key):
+    """The reference ships the coefficient masks its BHC drivers load
+    (utils/MaskWvlt<n>CircleL<L>D<D>.mat, written by its own utils/wvltMask.m
+    for Utils.getCircularMask(n); copied into tests/golden/wvltmask_golden.npz
+    by make_wvltmask_golden.py): the oracle's restatement of both reproduces
+    them bit for bit, the 6-tap filter included."""
+    z = np.load(MASKS)
+    n, L, D, ref = reference_mask(z, key)
+    assert np.array_equal(W.wvlt_mask(W.circular_mask(n), W.daubcqf(D), L), ref)
