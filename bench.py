@@ -308,7 +308,7 @@ def our_arm(args):
     shared = shared_roof(prof, kname, kms, clk.get("sm_mhz"))
 
     bhc_line = batch_line = extras_line = loop_line = None
-    if args.legs == "all":
+    if args.legs in ("all", "bhc"):
         # BHC gradient iterations on the polychromatic model's own configuration
         # (fan 1024^2, 720 views, 1024 bins, J = 20) and on the 2048^2 geometry
         g3 = ct.Geometry(*geometry_tuple(BHC_WORKLOAD))
@@ -318,6 +318,7 @@ def our_arm(args):
                     "fan_2048": bhc_leg(ct, g, pr, flush, stream, max(3, args.steps // 2), BHC["J"],
                                         "fan 2048^2, 1440 views, 2048 bins, d=8192 px")}
         pr3.close()
+    if args.legs == "all":
         batch_line = batch_leg(ct, flush, stream, max(3, args.steps // 2))
         extras_line = extras_leg(ct, g, pr, flush, stream, max(3, args.steps // 2))
         if args.loop_iters > 0:
@@ -889,8 +890,9 @@ def main():
     ap.add_argument("--loop-geometry", default="2048", choices=["2048", "1024"],
                     help="reconstruction leg on the 2048^2 workload (config 5) or on the "
                          "1024^2 configuration of the polychromatic model (smaller, for profiling)")
-    ap.add_argument("--legs", default="all", choices=["all", "projector", "geometries"],
+    ap.add_argument("--legs", default="all", choices=["all", "projector", "bhc", "geometries"],
                     help="projector: the headline step and its end-to-end run only (for profiling); "
+                         "bhc: the same plus the BHC gradient-iteration legs; "
                          "geometries: forward and backprojection times on each configuration's geometry")
     ap.add_argument("--selftest", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
