@@ -130,9 +130,12 @@ struct ctprj_plan {
     ctprj::DetEntry *d_det;
     float4 *d_quad;           // scratch: quad image, quad_elems(n) float4
     unsigned long long *d_count;
-    // FBP: ramp-filter taps (2*prjWidth) and filtered-sinogram scratch
+    // FBP: ramp-filter taps and pre-weights (2*prjWidth), then, where the rows
+    // are filtered by FFTs, the twiddles and response of the 2^fbp_log-point
+    // transform; filtered-sinogram scratch
     float *d_ramp;
     float *d_fsino;
+    int fbp_log;
     // MATLAB-layout entry points: image and sinogram scratch (allocated on first use)
     float *d_mimg;
     float *d_msino;

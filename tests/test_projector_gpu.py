@@ -109,6 +109,20 @@ def test_against_fp64_oracle_on_signed_and_phantom_inputs(name):
     assert rel(host(pr.fbp(dev(y))), oracle.fbp(g, y.astype(np.float64))) < 1e-4
 
 
+@pytest.mark.parametrize("g", [ct.Geometry(64, 4096, 7, 16, 1.0, 1.0, 0.0),
+                               ct.Geometry(64, 4097, 7, 16, 1.0, 1.0, 20000.0)], ids=["par4096", "fan4097"])
+def test_fbp_filter_on_both_sides_of_the_fft_limit(g):
+    """Rows of up to 4096 detectors are filtered by FFTs (8192 points, 64 KB of
+    shared memory a block, two views per transform), longer rows by the
+    Toeplitz kernel; both against the FP64 oracle's FFT filter, with an odd
+    view count (one block holds a single view)."""
+    rng = np.random.default_rng(4)
+    pr = ct.Projector(g)
+    y = rng.standard_normal((g.np, g.prjWidth)).astype(np.float32)
+    assert rel(host(pr.fbp(dev(y))), oracle.fbp(g, y.astype(np.float64))) < 1e-4
+    pr.close()
+
+
 @pytest.mark.parametrize("name", ["par256", "fan512"])
 def test_adjoint_dot_product(name):
     """<A x, y> = <x, A^T y>, normalised by |Ax| |y| (the reference pair itself
