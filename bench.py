@@ -772,9 +772,10 @@ def issue_roof(prof, kname, kms, sm_mhz, updates):
 
 
 def geometries_arm(args):
-    """Forward and backprojection times per geometry (CUDA events around each
-    launch on the launching stream, the 512 MiB L2 flush before each; median
-    of --steps launches after --warmup), one GPU."""
+    """Forward, backprojection and FBP (ramp filter + weighted backprojection)
+    times per geometry (CUDA events around each launch on the launching stream,
+    the 512 MiB L2 flush before each; median of --steps launches after
+    --warmup), one GPU."""
     import torch
     import imgrecsrc_b200 as ct
     torch.cuda.set_device(0)
@@ -790,7 +791,7 @@ def geometries_arm(args):
         s = torch.empty(g.np, g.prjWidth, device="cuda")
         b = torch.empty(g.n, g.n, device="cuda")
         res = {}
-        for kind in ("fwd_ms", "bwd_ms"):
+        for kind in ("fwd_ms", "bwd_ms", "fbp_ms"):
             ts = []
             for it in range(max(3, args.warmup) + args.steps):
                 flush.zero_()
@@ -798,8 +799,10 @@ def geometries_arm(args):
                 e0.record(stream)
                 if kind == "fwd_ms":
                     pr.forward(x, out=s)
-                else:
+                elif kind == "bwd_ms":
                     pr.backward(y, out=b)
+                else:
+                    pr.fbp(y, out=b)
                 e1.record(stream)
                 torch.cuda.synchronize()
                 if it >= max(3, args.warmup):
@@ -893,7 +896,7 @@ def main():
     ap.add_argument("--legs", default="all", choices=["all", "projector", "bhc", "geometries"],
                     help="projector: the headline step and its end-to-end run only (for profiling); "
                          "bhc: the same plus the BHC gradient-iteration legs; "
-                         "geometries: forward and backprojection times on each configuration's geometry")
+                         "geometries: forward, backprojection and FBP times on each configuration's geometry")
     ap.add_argument("--selftest", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.gpus < 1:
