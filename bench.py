@@ -56,6 +56,14 @@ GEOMETRIES = {
 }
 
 
+def run_config(world):
+    """The `config` of both arms' lines, identical by construction: the
+    workload, how the timed steps treat the GPU's L2, and the process layout."""
+    return dict(WORKLOAD, l2="GPU arm: 512 MiB written between timed steps (L2 flushed); "
+                             "reference arm: the same steps on the host cores",
+                parallelism="replicas" if world > 1 else "single GPU")
+
+
 def geometry_tuple(w):
     return (w["n"], w["prjWidth"], w["np"], w["prjFull"], w["dSize"], w["effectiveRate"], w["d"])
 
@@ -192,12 +200,12 @@ def reference_arm(args):
         raise SystemExit("bench.py: %d ranks started for --gpus %d" % (world, args.gpus))
     if rank != 0:
         return
-    steps, warmup = max(1, args.steps), max(0, args.warmup)
+    steps, warmup = max(1, args.steps), max(3, args.warmup)
     v, t, info = cpu_reference_run(steps, warmup)
     line = {"metric": METRIC, "value": v, "unit": "Gray-px/s", "n_gpus": args.gpus,
             "steps": steps, "warmup": warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ellipse phantom)",
-            "impl": "reference", "config": dict(WORKLOAD),
+            "impl": "reference", "config": run_config(world),
             "cpu_baseline": dict(value=v, unit="Gray-px/s", **info),
             "e2e": {"value": v, "unit": "Gray-px/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -374,10 +382,9 @@ def our_arm(args):
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t_max,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded ellipse phantom)",
-        "config": dict(WORKLOAD, l2="flushed between timed steps (512 MiB write)",
-                       parallelism="replicas" if world > 1 else "single GPU",
-                       updates_per_step={"forward": nnz_f, "backward": nnz_b},
-                       fwd_ms=fwd_ms, bwd_ms=bwd_ms),
+        "config": run_config(world),
+        "updates_per_step": {"forward": nnz_f, "backward": nnz_b},
+        "pass_ms": {"forward": fwd_ms, "backward": bwd_ms},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,
@@ -417,8 +424,8 @@ def summary(line):
     """Headline figures of every leg in one short object (rounded)."""
     def r(v, k=4):
         return None if v is None else float("%.*g" % (k, v))
-    c = line["config"]
-    out = {"fwd_ms": r(c["fwd_ms"]), "bwd_ms": r(c["bwd_ms"]), "gray_px_s": r(line["value"]),
+    c = line["pass_ms"]
+    out = {"fwd_ms": r(c["forward"]), "bwd_ms": r(c["backward"]), "gray_px_s": r(line["value"]),
            "e2e_gray_px_s": r(line["e2e"]["value"]),
            "issue_frac": r((line["roofline"].get("issue") or {}).get("frac"), 3)}
     if line["roofline"].get("shared"):

@@ -82,3 +82,27 @@ def test_rank_count_must_match_gpus():
                         "--steps", "1"], capture_output=True, text=True, env=env, timeout=120)
     assert r.returncode != 0
     assert "1 ranks started for --gpus 2" in r.stderr
+
+
+def test_reference_arm_line_carries_the_shared_config(monkeypatch, capsys):
+    """Both arms print the same `config` (bench.run_config) and at least three
+    warm-up steps, so the two lines describe one workload; the reference's CPU
+    projector is stubbed here (its timing is not under test)."""
+    import argparse
+    import json
+    sys.path.insert(0, ROOT)
+    import bench
+    seen = {}
+
+    def fake_run(steps, warmup):
+        seen.update(steps=steps, warmup=warmup)
+        return 4.0, 6.5, {"kind": "reference", "cores": 16, "sample": "stub"}
+    monkeypatch.setattr(bench, "cpu_reference_run", fake_run)
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
+        monkeypatch.delenv(k, raising=False)
+    bench.reference_arm(argparse.Namespace(gpus=1, steps=20, warmup=1))
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["config"] == bench.run_config(1)
+    assert line["config"]["n"] == 2048 and line["config"]["np"] == 1440
+    assert line["steps"] == 20 and line["warmup"] == 3 and seen == {"steps": 20, "warmup": 3}
+    assert line["impl"] == "reference" and line["e2e"]["value"] == line["value"]
