@@ -1445,7 +1445,13 @@ __device__ __forceinline__ void backward_tile(const BwdParams &p, int tile,
                     const float qe = FAN ? t.qec - dv : 0.0f;
                     // the detector under the pixel centre, in staged units
                     const float tc = FAN ? __fdividef(dFs * u, qe) : u * invdS;
-                    const int ks = WIN == 3 ? __float2int_rn(tc) : __float2int_rd(tc);
+                    // nearest detector, half to even as __float2int_rn, by an FP32
+                    // add: for |tc| < 2^22 (staged units: |tc| < the row length)
+                    // tc + 1.5 * 2^23 lies in [2^23, 2^24), where the add rounds to
+                    // an integer, so its low mantissa bits are that integer (one
+                    // arithmetic op instead of a conversion on the XU pipe: 0.5 %
+                    // at the 2048^2 fan workload, 1.5-2 % at 512^2 and 256^2)
+                    const int ks = WIN == 3 ? __float_as_int(tc + 12582912.0f) - 0x4B400000 : __float2int_rd(tc);
                     const int k0 = min(max(ks - 1 - t.klo, 0), t.nseg - WIN);
                     const float fbpw = FBP ? __fdividef(g.dF, qe) * __fdividef(g.dF, qe) : 1.0f;
                     const FootprintV fpar = FAN ? FootprintV{} : pfs[iv];
