@@ -106,3 +106,18 @@ def test_reference_arm_line_carries_the_shared_config(monkeypatch, capsys):
     assert line["config"]["n"] == 2048 and line["config"]["np"] == 1440
     assert line["steps"] == 20 and line["warmup"] == 3 and seen == {"steps": 20, "warmup": 3}
     assert line["impl"] == "reference" and line["e2e"]["value"] == line["value"]
+
+
+def test_summary_reads_the_line_layout():
+    """bench.summary() on a line of the GPU arm's layout (pass times beside the
+    shared config, optional legs absent): the headline figures come out rounded."""
+    sys.path.insert(0, ROOT)
+    import bench
+    line = {"value": 3158.04, "config": bench.run_config(1),
+            "pass_ms": {"forward": 3.5721, "backward": 4.5903},
+            "e2e": {"value": 2947.2}, "roofline": {"issue": {"frac": 0.6512}, "shared": {"frac": 0.8013}},
+            "cpu_baseline": {"value": 3.87}}
+    out = bench.summary(line)
+    assert out["fwd_ms"] == 3.572 and out["bwd_ms"] == 4.59 and out["gray_px_s"] == 3158.0
+    assert out["e2e_gray_px_s"] == 2947.0 and out["issue_frac"] == 0.651 and out["shared_frac"] == 0.801
+    assert out["cpu_gray_px_s"] == 3.87 and "bhc_fan_2048" not in out
